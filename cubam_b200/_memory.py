@@ -1,0 +1,32 @@
+"""GPU memory: how much to read at a time, and the pool.
+
+Mirrors ``src/cubam/_memory.py``: the chunk policy is the same (256 MB,
+halved while 64 chunks do not fit in free GPU memory, never below 32 MB).
+Buffers come from PyTorch's caching allocator, which is already a
+stream-ordered pool, so :func:`memory_pool` only has to exist for callers
+written against cubam.
+"""
+
+from __future__ import annotations
+
+from contextlib import contextmanager
+
+import torch
+
+#: Peak GPU memory of the reader is a small multiple of the compressed chunk
+_CHUNK_SHARE = 64
+
+
+def auto_chunk_bytes() -> int:
+    """Compressed bytes to read per chunk (``src/cubam/_memory.py:11-23``)."""
+    free, _ = torch.cuda.mem_get_info()
+    size = 256 << 20
+    while size > 32 << 20 and size * _CHUNK_SHARE > free:
+        size //= 2
+    return size
+
+
+@contextmanager
+def memory_pool():
+    """Kept for cubam's API (``src/cubam/_memory.py:27-45``): PyTorch's caching allocator is the pool."""
+    yield

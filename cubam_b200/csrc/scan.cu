@@ -1,0 +1,312 @@
+// BGZF member scan on B200: replaces bgzf_candidates, bgzf_sizes, the chain and the checks of
+// _inflate_blocks (src/cubam/_kernels.py:69-89, src/cubam/_kernels.py:662-702,
+// src/cubam/bgzf.py:542-586).
+//
+//  1. k_scan_count: each thread loads 16 bytes with one 128-bit load; __vcmpeq4 finds 0x1f bytes
+//     (about 1 in 256 in compressed data) and only those offsets get the full header test.  The
+//     count of every 4 KB tile goes to the workspace.
+//  2. k_scan_tiles: one block turns the tile counts into tile offsets (prefix sum).
+//  3. k_scan_write: tiles with candidates are tested again and their offsets written in order
+//     (block prefix sum of the per-thread counts); no sort is needed.
+//  4. k_scan_finish: one block keeps the chain from offset 0 (all candidates in the usual case,
+//     otherwise a walk), applies the reference's checks in the reference's order and writes the
+//     inflate jobs of the non-empty members with their output offsets (prefix sum of ISIZE).
+
+#include "common.cuh"
+
+namespace cb {
+namespace scan {
+
+constexpr int NT = 256;
+constexpr int TILE = NT * 16;
+constexpr int FIN_NT = 1024;
+constexpr long long MAX_ISIZE = 1 << 16;
+
+struct Ws {
+    uint32_t* tile_count;
+    int64_t* tile_off;
+    int64_t* cand;
+    uint8_t* keep;
+    int64_t* meta;  // [0] candidates, [1] status
+    long long ntiles, cap;
+};
+
+__host__ __device__ inline long long n_tiles(const uint8_t* buf, long long n) {
+    uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
+    long long chunks = (long long)(((uintptr_t)buf + n + 15 - base) >> 4);
+    return (chunks + NT - 1) / NT + 1;
+}
+
+__host__ __device__ inline long long cand_cap(long long n) { return n / 28 + 1024; }
+
+__host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+__host__ __device__ inline Ws carve(void* ws, const uint8_t* buf, long long n) {
+    Ws w;
+    w.ntiles = n_tiles(buf, n);
+    w.cap = cand_cap(n);
+    uint8_t* p = reinterpret_cast<uint8_t*>(ws);
+    w.meta = reinterpret_cast<int64_t*>(p);
+    p += 256;
+    w.tile_count = reinterpret_cast<uint32_t*>(p);
+    p += align256(w.ntiles * 4);
+    w.tile_off = reinterpret_cast<int64_t*>(p);
+    p += align256(w.ntiles * 8);
+    w.cand = reinterpret_cast<int64_t*>(p);
+    p += align256(w.cap * 8);
+    w.keep = p;
+    return w;
+}
+
+__host__ inline size_t ws_bytes(long long n) {
+    // worst case alignment of buf shifts the tile count by one
+    long long ntiles = (n + 15 + 16) / 16 / NT + 2;
+    long long cap = cand_cap(n);
+    return 256 + align256(ntiles * 4) + align256(ntiles * 8) + align256(cap * 8) + align256(cap) + 256;
+}
+
+__device__ __forceinline__ bool member_at(const uint8_t* b, long long n, long long o) {
+    if (o < 0 || o + 18 > n) return false;
+    if (b[o] != 31 || b[o + 1] != 139 || b[o + 2] != 8 || b[o + 3] != 4) return false;
+    if (b[o + 10] != 6 || b[o + 11] != 0 || b[o + 12] != 66 || b[o + 13] != 67 || b[o + 14] != 2 || b[o + 15] != 0)
+        return false;
+    long long bs = (long long)ld_u16(b, o + 16) + 1;
+    return bs >= 26 && o + bs <= n;
+}
+
+// Bit mask (bit k = offset start + k) of the candidates in 16-byte chunk c of the aligned view of buf.
+__device__ __forceinline__ uint32_t chunk_candidates(const uint8_t* buf, long long n, long long c) {
+    uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
+    uintptr_t a = base + 16 * (uintptr_t)c;
+    long long start = (long long)(a - (uintptr_t)buf);
+    if (start >= n || start + 16 <= 0) return 0;
+    uint32_t w[4];
+    if (start >= 0 && start + 16 <= n) {
+        uint4 v = __ldg(reinterpret_cast<const uint4*>(a));
+        w[0] = v.x;
+        w[1] = v.y;
+        w[2] = v.z;
+        w[3] = v.w;
+    } else {
+        for (int k = 0; k < 4; k++) {
+            uint32_t x = 0;
+            for (int t = 0; t < 4; t++) {
+                long long o = start + 4 * k + t;
+                if (o >= 0 && o < n) x |= (uint32_t)buf[o] << (8 * t);
+            }
+            w[k] = x;
+        }
+    }
+    uint32_t mask = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        uint32_t eq = __vcmpeq4(w[k], 0x1f1f1f1fu);
+        while (eq) {
+            int t = (__ffs(eq) - 1) >> 3;
+            eq &= ~(0xffu << (8 * t));
+            long long o = start + 4 * k + t;
+            if (member_at(buf, n, o)) mask |= 1u << (4 * k + t);
+        }
+    }
+    return mask;
+}
+
+__global__ void __launch_bounds__(NT) k_scan_count(const uint8_t* buf, long long n, Ws w) {
+    __shared__ uint32_t red[NT / 32];
+    for (long long t = blockIdx.x; t < w.ntiles; t += gridDim.x) {
+        uint32_t c = __popc(chunk_candidates(buf, n, t * NT + threadIdx.x));
+        for (int d = 16; d; d >>= 1) c += __shfl_down_sync(FULL, c, d);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t s = 0;
+            for (int i = 0; i < NT / 32; i++) s += red[i];
+            w.tile_count[t] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Exclusive prefix sum of the tile counts (one block); meta[0] = total, meta[1] = status.
+__global__ void __launch_bounds__(FIN_NT) k_scan_tiles(Ws w, long long too_many) {
+    __shared__ int64_t sm[33];
+    int64_t carry = 0;
+    for (long long b = 0; b < w.ntiles; b += FIN_NT) {
+        long long i = b + threadIdx.x;
+        int64_t v = i < w.ntiles ? (int64_t)w.tile_count[i] : 0;
+        int64_t tot;
+        int64_t x = block_exclusive_scan<FIN_NT>(v, tot, sm);
+        if (i < w.ntiles) w.tile_off[i] = carry + x;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) {
+        w.meta[0] = carry;
+        w.meta[1] = carry > too_many ? CB_ERR_TOO_MANY : (carry > w.cap ? CB_ERR_CAPACITY : CB_OK);
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_scan_write(const uint8_t* buf, long long n, Ws w) {
+    __shared__ int64_t sm[33];
+    if (w.meta[1] != CB_OK) return;
+    for (long long t = blockIdx.x; t < w.ntiles; t += gridDim.x) {
+        if (w.tile_count[t] == 0) continue;
+        long long c = t * NT + threadIdx.x;
+        uint32_t mask = chunk_candidates(buf, n, c);
+        int64_t tot;
+        int64_t pos = w.tile_off[t] + block_exclusive_scan<NT>((int64_t)__popc(mask), tot, sm);
+        long long start = (long long)(((uintptr_t)buf & ~(uintptr_t)15) + 16 * (uintptr_t)c - (uintptr_t)buf);
+        while (mask) {
+            int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            w.cand[pos++] = start + k;
+        }
+    }
+}
+
+__device__ __forceinline__ long long lower_bound(const int64_t* a, long long m, long long x) {
+    long long lo = 0, hi = m;
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(FIN_NT) k_scan_finish(const uint8_t* buf, long long n, int eof, long long out_base,
+                                                       cb_member_job* jobs, long long jobs_cap,
+                                                       cb_scan_summary* summary, Ws w) {
+    __shared__ int64_t sm[33];
+    __shared__ int s_breaks;
+    __shared__ long long s_last;
+    const long long m = w.meta[0];
+    int status = (int)w.meta[1];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_breaks = 0;
+        s_last = -1;
+        summary->n_members = 0;
+        summary->n_jobs = 0;
+        summary->used = 0;
+        summary->total_out = 0;
+        summary->n_candidates = m;
+        summary->chained = 1;
+    }
+    __syncthreads();
+    if (status == CB_OK && m == 0 && eof && n > 0) status = CB_ERR_TRUNCATED;
+    if (status == CB_OK && m > 0 && w.cand[0] != 0) status = CB_ERR_NO_CHAIN;
+    if (status != CB_OK || m == 0) {
+        if (tid == 0) summary->status = status;
+        return;
+    }
+    // fast path: every candidate ends where the next starts
+    int local = 0;
+    for (long long i = tid; i + 1 < m; i += FIN_NT) {
+        long long c = w.cand[i];
+        long long bs = (long long)ld_u16(buf, c + 16) + 1;
+        if (c + bs != w.cand[i + 1]) local = 1;
+    }
+    if (local) atomicOr(&s_breaks, 1);
+    __syncthreads();
+    if (s_breaks) {
+        for (long long i = tid; i < m; i += FIN_NT) w.keep[i] = 0;
+        __syncthreads();
+        if (tid == 0) {
+            long long i = 0;
+            for (;;) {
+                w.keep[i] = 1;
+                long long c = w.cand[i];
+                long long nx = c + (long long)ld_u16(buf, c + 16) + 1;
+                long long j = lower_bound(w.cand, m, nx);
+                if (j >= m || w.cand[j] != nx) break;
+                i = j;
+            }
+            summary->chained = 0;
+        }
+        __syncthreads();
+    }
+    const bool all = s_breaks == 0;
+    // last kept member -> used
+    for (long long i = tid; i < m; i += FIN_NT)
+        if (all || w.keep[i]) atomicMax(reinterpret_cast<unsigned long long*>(&s_last), (unsigned long long)i);
+    __syncthreads();
+    const long long last = s_last;
+    const long long used = w.cand[last] + (long long)ld_u16(buf, w.cand[last] + 16) + 1;
+    if (eof && used != n) {
+        if (tid == 0) summary->status = CB_ERR_TRUNCATED;
+        return;
+    }
+    // checks and jobs
+    int bad = 0;
+    int64_t carry_jobs = 0, carry_out = 0, kept = 0;
+    for (long long b = 0; b <= last; b += FIN_NT) {
+        long long i = b + tid;
+        int64_t is_job = 0, isz = 0;
+        long long c = 0, bs = 0;
+        if (i <= last && (all || w.keep[i])) {
+            c = w.cand[i];
+            bs = (long long)ld_u16(buf, c + 16) + 1;
+            isz = (int64_t)ld_u32(buf, c + bs - 4);
+            kept++;
+            if (isz > MAX_ISIZE) bad = 1;
+            if (isz == 0 && (bs != 28 || buf[c + 18] != 3 || buf[c + 19] != 0)) bad = 1;
+            is_job = isz > 0 && isz <= MAX_ISIZE;
+        }
+        int64_t tj, to;
+        int64_t xj = block_exclusive_scan<FIN_NT>(is_job, tj, sm);
+        int64_t xo = block_exclusive_scan<FIN_NT>(is_job ? isz : 0, to, sm);
+        if (is_job) {
+            long long k = carry_jobs + xj;
+            if (k < jobs_cap) {
+                cb_member_job j;
+                j.in = buf + c + 18;
+                j.out_off = out_base + carry_out + xo;
+                j.in_len = (uint32_t)(bs - 26);
+                j.isize = (uint32_t)isz;
+                j.crc = ld_u32(buf, c + bs - 8);
+                j.reserved = 0;
+                jobs[k] = j;
+            }
+        }
+        carry_jobs += tj;
+        carry_out += to;
+    }
+    if (bad) atomicOr(&s_breaks, 2);
+    __syncthreads();
+    int64_t tot_kept;
+    block_exclusive_scan<FIN_NT>(kept, tot_kept, sm);
+    if (tid == 0) {
+        int st = (s_breaks & 2) ? CB_ERR_CORRUPT_BLOCK : (carry_jobs > jobs_cap ? CB_ERR_CAPACITY : CB_OK);
+        summary->status = st;
+        summary->n_members = tot_kept;
+        summary->n_jobs = carry_jobs;
+        summary->used = used;
+        summary->total_out = carry_out;
+    }
+}
+
+}  // namespace scan
+}  // namespace cb
+
+using namespace cb;
+
+int cb_set_error(cudaError_t e);  // abi.cu
+
+extern "C" size_t cb_scan_workspace_bytes(int64_t n) { return scan::ws_bytes(n < 0 ? 0 : n); }
+
+extern "C" int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off, cb_member_job* jobs,
+                               int64_t cap, cb_scan_summary* summary, void* workspace, size_t workspace_bytes,
+                               void* stream) {
+    if (n < 0 || !summary || !workspace || (n > 0 && !buf) || cap < 0) return CB_ERR_ARG;
+    if (workspace_bytes < scan::ws_bytes(n)) return CB_ERR_CAPACITY;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    scan::Ws w = scan::carve(workspace, buf, n);
+    int sms = cb_device_sm_count();
+    long long grid = w.ntiles < (long long)sms * 8 ? w.ntiles : (long long)sms * 8;
+    if (grid < 1) grid = 1;
+    scan::k_scan_count<<<(unsigned)grid, scan::NT, 0, s>>>(buf, n, w);
+    scan::k_scan_tiles<<<1, scan::FIN_NT, 0, s>>>(w, scan::cand_cap(n));
+    scan::k_scan_write<<<(unsigned)grid, scan::NT, 0, s>>>(buf, n, w);
+    scan::k_scan_finish<<<1, scan::FIN_NT, 0, s>>>(buf, n, eof, out_base_off, jobs, cap, summary, w);
+    return cb_set_error(cudaGetLastError());
+}

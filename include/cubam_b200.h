@@ -1,0 +1,168 @@
+/* cubam_b200: the BAM reader hot path on NVIDIA B200 (sm_100a), as a C ABI.
+ *
+ * Plain pointers and sizes only.  Every `const uint8_t* / int64_t* ...` data
+ * argument is DEVICE memory unless its comment says "host".  `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Every
+ * entry point returns CB_OK (0) or a CB_ERR_* code; device-side findings
+ * (corrupt data) are written to the summary structs, which live in device
+ * memory and are read by the caller after synchronising the stream.
+ *
+ * Each entry point cites the interface of cubam (LouisFaure/cubam) it
+ * replaces, as path:line inside that project.
+ */
+#ifndef CUBAM_B200_H
+#define CUBAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+enum {
+    CB_OK = 0,
+    CB_ERR_TRUNCATED = 1,     /* "Truncated BGZF file: the last block is incomplete" (src/cubam/bgzf.py:557,567) */
+    CB_ERR_NO_CHAIN = 2,      /* "No valid block or record where one was expected: the data is corrupt" (src/cubam/_kernels.py:688) */
+    CB_ERR_CORRUPT_BLOCK = 3, /* "Corrupt BGZF block" (src/cubam/bgzf.py:576,584) */
+    CB_ERR_INFLATE = 4,       /* "Corrupt BGZF block: it does not inflate to the size in its trailer" (src/cubam/bgzf.py:611) */
+    CB_ERR_CRC = 5,           /* CRC32 of a member differs from its trailer (cubam does not check; docs/reading.md:48-51) */
+    CB_ERR_TOO_MANY = 6,      /* "Too many candidates: the data is corrupt" (src/cubam/_kernels.py:671) */
+    CB_ERR_CAPACITY = 7,      /* an output or workspace buffer given by the caller is too small */
+    CB_ERR_CUDA = 8,          /* a CUDA call failed (cb_last_error() has the text) */
+    CB_ERR_ARG = 9,           /* invalid argument */
+    CB_ERR_TIMEOUT = 10       /* a bounded device-side wait ran out */
+};
+
+/* One BGZF member to inflate: DEFLATE payload at `in` (in_len bytes), output
+ * at out_base + out_off (isize bytes), CRC32 from the member's trailer. */
+typedef struct cb_member_job {
+    const uint8_t* in;
+    int64_t out_off;
+    uint32_t in_len;
+    uint32_t isize;
+    uint32_t crc;
+    uint32_t reserved;
+} cb_member_job;
+
+/* Result of cb_scan_members (device memory). */
+typedef struct cb_scan_summary {
+    int64_t n_members;    /* chained members, empty ones included */
+    int64_t n_jobs;       /* non-empty members = inflate jobs written */
+    int64_t used;         /* compressed bytes used: end of the last chained member */
+    int64_t total_out;    /* sum of ISIZE of the jobs */
+    int64_t n_candidates; /* header matches before chaining */
+    int32_t status;       /* CB_OK or CB_ERR_* */
+    int32_t chained;      /* 1 when every candidate was on the chain (no pointer jumping) */
+} cb_scan_summary;
+
+/* Result of cb_inflate (device memory). */
+typedef struct cb_inflate_summary {
+    int32_t status;       /* CB_OK, or the worst CB_ERR_* of the jobs */
+    int32_t reserved;
+    int64_t n_bad;        /* jobs that failed */
+    int64_t first_bad;    /* lowest failing job index, or -1 */
+} cb_inflate_summary;
+
+/* Result of cb_record_chain (device memory). */
+typedef struct cb_chain_summary {
+    int64_t n_records;    /* records on the chain from offset 0 */
+    int64_t tail;         /* where the record after the last one starts (0 when there is none) */
+    int64_t n_candidates; /* offsets that pass the record predicate */
+    int32_t status;       /* CB_OK, CB_ERR_NO_CHAIN, CB_ERR_TOO_MANY or CB_ERR_CAPACITY */
+    int32_t chained;      /* 1 when every candidate was on the chain */
+} cb_chain_summary;
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Version string of the library. */
+const char* cb_version(void);
+/* Text of the last CB_ERR_CUDA / CB_ERR_ARG of the calling thread. */
+const char* cb_last_error(void);
+/* Number of SMs of the current device (for sizing persistent grids). */
+int cb_device_sm_count(void);
+
+/* ---- BGZF member scan: replaces bgzf_candidates + bgzf_sizes + chain + the checks of _inflate_blocks
+ *      (src/cubam/_kernels.py:69-89, src/cubam/_kernels.py:662-702, src/cubam/bgzf.py:542-586) ---------- */
+
+/* Workspace bytes cb_scan_members needs for an n-byte buffer. */
+size_t cb_scan_workspace_bytes(int64_t n);
+
+/* Scan buf[0:n) (starting at a member) for BGZF members with 128-bit loads and warp
+ * ballots, keep the chain from offset 0, check it as the reference does (truncation when
+ * `eof`, ISIZE <= 65536, the empty-member rule) and write one job per non-empty member to
+ * jobs[0:cap) with out_off = out_base_off + the prefix sum of ISIZE.  The result, including
+ * the status, goes to *summary (device). */
+int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off, cb_member_job* jobs, int64_t cap,
+                    cb_scan_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Inflate: replaces nvcompBatchedDeflateDecompressAsync and the status/size check
+ *      (src/cubam/bgzf.py:587-611); adds the CRC32 check ---------------------------------------- */
+
+/* Workspace bytes of cb_inflate. */
+size_t cb_inflate_workspace_bytes(void);
+
+/* Inflate jobs[0:n_jobs) (raw DEFLATE: stored, fixed and dynamic Huffman blocks) into
+ * out_base + jobs[i].out_off, one warp per member, with a persistent grid that takes
+ * members from a work queue.  When d_n_jobs is not NULL the job count is read from device
+ * memory (n_jobs is then the capacity).  Each member must give exactly isize bytes; with
+ * check_crc its CRC32 must match.  job_status (device, may be NULL) gets a code per job. */
+int cb_inflate(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
+               uint32_t* job_status, cb_inflate_summary* summary, void* workspace, size_t workspace_bytes,
+               void* stream);
+
+/* ---- Record chain: replaces record_candidates + record_ends + chain (src/cubam/_kernels.py:250-289,
+ *      src/cubam/bam.py:403-418) --------------------------------------------------------------- */
+
+size_t cb_record_chain_workspace_bytes(int64_t n);
+
+/* Offsets of the complete records of data[0:n) on the chain from offset 0, under the reference's
+ * record predicate (is_record, src/cubam/_kernels.py:250-278).  Writes offsets[0:cap) and *summary. */
+int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, int64_t* offsets, int64_t cap,
+                    cb_chain_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Columns: replaces decode_fixed (src/cubam/_kernels.py:292-319, src/cubam/bam.py:269-288) ---- */
+
+int cb_decode_fixed(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
+                    int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
+                    int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, void* stream);
+
+/* ---- Tags: replaces find_tag, one launch per tag (src/cubam/_kernels.py:334-388, src/cubam/bam.py:184-208).
+ * One aux walk per record finds k tags (k <= 16); `names` (host) holds 2k characters.  Output is
+ * tag-major: type[t * n + i] etc. --------------------------------------------------------------- */
+int cb_find_tags(const uint8_t* data, const int64_t* offsets, int64_t n, const char* names, int32_t k,
+                 uint8_t* type, int64_t* voff, int32_t* vlen, int64_t* value, void* stream);
+
+/* ---- On-request decoders (src/cubam/bam.py:221-400, src/cubam/_kernels.py:322-620) -------------- */
+
+/* FNV-1a 64 of read names (name_hash, src/cubam/_kernels.py:322-330). */
+int cb_name_hash(const uint8_t* data, const int64_t* offsets, int64_t n, uint64_t* out, void* stream);
+/* FNV-1a 64 of spans, 0 where vlen < 0 (hash_spans, src/cubam/_kernels.py:532-540). */
+int cb_hash_spans(const uint8_t* data, const int64_t* voff, const int32_t* vlen, int64_t n, uint64_t* out,
+                  void* stream);
+/* [ACGT]{1,24}(-[0-9]{1,3})? packed in 64 bits (pack_acgt, src/cubam/_kernels.py:544-571). */
+int cb_pack_acgt(const uint8_t* data, const int64_t* voff, const int32_t* vlen, int64_t n, uint64_t* out,
+                 uint8_t* ok, void* stream);
+/* Strings of packed codes at dst_off (unpack_acgt, src/cubam/_kernels.py:607-620). */
+int cb_unpack_acgt(const uint64_t* codes, const int64_t* dst_off, int64_t n, uint8_t* chars, void* stream);
+/* Aligned bases M/=/X (aligned_len, src/cubam/_kernels.py:391-403). */
+int cb_aligned_length(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* out, void* stream);
+/* Aligned blocks, two passes as the reference (blocks, src/cubam/_kernels.py:408-437):
+ * fill = 0 counts into cnt; fill = 1 writes rec/start/end from first[i]. */
+int cb_blocks(const uint8_t* data, const int64_t* offsets, int64_t n, int split_del, int fill, const int64_t* first,
+              int32_t* cnt, int64_t* rec, int32_t* start, int32_t* end, void* stream);
+/* Base of read rec[j] at reference position refpos[j] (base_at, src/cubam/_kernels.py:498-529). */
+int cb_base_at(const uint8_t* data, const int64_t* offsets, const int64_t* rec, const int32_t* refpos, int64_t m,
+               int8_t* out, void* stream);
+/* dst[dst_off[i]:+size[i]] = src[src_off[i]:+size[i]] (copy_spans, src/cubam/_kernels.py:34-43). */
+int cb_copy_spans(const uint8_t* src, uint8_t* dst, const int64_t* src_off, const int64_t* dst_off,
+                  const int64_t* size, int64_t n, void* stream);
+/* Record sizes incl. the length field (record_sizes, src/cubam/bam.py:308-315). */
+int cb_record_sizes(const uint8_t* data, const int64_t* offsets, int64_t n, int64_t* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUBAM_B200_H */

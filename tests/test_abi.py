@@ -1,0 +1,48 @@
+"""The C ABI: the library loads on a machine without a GPU and exports every entry point of include/*.h."""
+
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared() -> list[str]:
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(cb_[a-z_0-9]+)\s*\(", text, flags=re.M)
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from cubam_b200 import _lib
+
+    names = declared()
+    assert len(names) >= 20
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(_lib.exported_symbols()) | set(), set(names) - set(_lib.exported_symbols())
+
+
+def test_no_gpu_calls_needed_for_sizes():
+    from cubam_b200 import _lib
+
+    assert _lib.lib.cb_version().startswith(b"cubam_b200")
+    assert _lib.lib.cb_scan_workspace_bytes(1 << 20) > (1 << 20) // 28 * 8
+    assert _lib.lib.cb_record_chain_workspace_bytes(1 << 20) > 0
+    assert _lib.lib.cb_inflate_workspace_bytes() >= 8
+    assert ctypes.sizeof(_lib.MemberJob) == 32
+    assert ctypes.sizeof(_lib.ScanSummary) == 48
+    assert ctypes.sizeof(_lib.InflateSummary) == 24
+    assert ctypes.sizeof(_lib.ChainSummary) == 32
+
+
+def test_bad_arguments_are_rejected_without_a_launch():
+    from cubam_b200 import _lib
+
+    assert _lib.lib.cb_scan_members(None, -1, 0, 0, None, 0, None, None, 0, None) == _lib.ARG
+    assert _lib.lib.cb_inflate(None, -1, None, None, 1, None, None, None, 0, None) == _lib.ARG
+    assert _lib.lib.cb_find_tags(None, None, 1, b"CB", 0, None, None, None, None, None) == _lib.ARG
+    assert _lib.lib.cb_decode_fixed(None, None, -5, *([None] * 11), None) == _lib.ARG

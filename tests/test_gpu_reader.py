@@ -1,0 +1,247 @@
+"""GPU parity of the reader against the golden vectors of the reference and the CPU oracle.
+
+Everything here calls the native library (``include/cubam_b200.h``) through
+``cubam_b200``; the expected values come from ``tests/golden/`` (made by the
+reference's own writer and reader code) and from ``oracle/bam_oracle.py``.
+"""
+
+import random
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+from golden_io import GOLDEN, TAGS, bam_cases, batches, meta
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+import cubam_b200  # noqa: E402
+from cubam_b200 import bgzf as G  # noqa: E402
+from oracle import bam_oracle as O  # noqa: E402
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def member(data: bytes, level: int = 6, strategy: int = zlib.Z_DEFAULT_STRATEGY, mem_level: int = 8) -> bytes:
+    c = zlib.compressobj(level, zlib.DEFLATED, -15, mem_level, strategy)
+    payload = c.compress(data) + c.flush()
+    bsize = 18 + len(payload) + 8
+    head = b"\x1f\x8b\x08\x04\x00\x00\x00\x00\x00\xff\x06\x00BC\x02\x00" + struct.pack("<H", bsize - 1)
+    return head + payload + struct.pack("<II", zlib.crc32(data) & 0xFFFFFFFF, len(data))
+
+
+@pytest.mark.parametrize(("name", "chunk"), bam_cases())
+def test_read_bam_matches_reference(tmp_path, name, chunk):
+    path = GOLDEN / name
+    got = list(cubam_b200.read_bam(path, chunk_bytes=chunk, piece=chunk // 2 + 1))
+    exp = batches(name, chunk)
+    assert len(got) == len(exp)
+    for b, e in zip(got, exp):
+        assert int(b.data.numel()) == e["data_size"]
+        assert _np(b.offset).tolist() == e["offset"].tolist()
+        for k in cubam_b200.RecordBatch.FIELDS:
+            col = _np(getattr(b, k))
+            assert col.dtype == e[k].dtype, k
+            assert col.tolist() == e[k].tolist(), k
+        assert _np(b.name_hash()).tolist() == e["name_hash"].tolist()
+        assert b.names().to_bytes_list() == e["names"]
+        assert _np(b.aligned_length()).tolist() == e["aligned_length"].tolist()
+        assert _np(b.five_prime()).tolist() == e["five_prime"].tolist()
+        assert _np(b.record_sizes()).tolist() == e["record_sizes"].tolist()
+        for split in (0, 1):
+            rec, start, end = b.blocks(split_deletions=bool(split))
+            assert _np(rec).tolist() == e[f"blocks{split}_rec"].tolist()
+            assert _np(start).tolist() == e[f"blocks{split}_start"].tolist()
+            assert _np(end).tolist() == e[f"blocks{split}_end"].tolist()
+        assert _np(b.base_at(e["base_rec"], e["base_pos"])).tolist() == e["base_at"].tolist()
+        tags = b.tags(*TAGS)
+        for t_name, t in zip(TAGS, tags):
+            single = b.tag(t_name)
+            p = f"tag_{t_name}_"
+            for tt in (t, single):
+                assert _np(tt.type).tolist() == e[p + "type"].tolist(), t_name
+                assert _np(tt.offset).tolist() == e[p + "offset"].tolist(), t_name
+                assert _np(tt.length).tolist() == e[p + "length"].tolist(), t_name
+                assert _np(tt.value).tolist() == e[p + "value"].tolist(), t_name
+            assert _np(t.hash()).tolist() == e[p + "hash"].tolist(), t_name
+            code, ok = t.packed()
+            assert _np(code).tolist() == e[p + "packed"].tolist(), t_name
+            assert _np(ok).tolist() == e[p + "packed_ok"].astype(bool).tolist(), t_name
+            assert t.strings().to_bytes_list() == e[p + "str"], t_name
+
+
+def test_take_flags_and_unpack():
+    (b,) = list(cubam_b200.read_bam(GOLDEN / "pairs.bam"))
+    sel = b.has_flags(all_of=1, none_of=0x400)
+    sub = b.take(sel)
+    assert len(sub) == int(sel.sum())
+    assert sub.data.data_ptr() == b.data.data_ptr()
+    (b2,) = list(cubam_b200.read_bam(GOLDEN / "mixed_b65280.bam", chunk_bytes=1 << 22))
+    code, ok = b2.tag("CB").packed()
+    s = cubam_b200.unpack_acgt(code[ok]).to_pylist()
+    full = [x.decode() for x, k in zip(b2.tag("CB").strings().to_bytes_list(), _np(ok)) if k]
+    assert s == full
+
+
+def test_header_and_empty_bam():
+    h = cubam_b200.BamHeader.read(GOLDEN / "empty.bam")
+    g = meta()["header"]["empty.bam"]
+    assert (h.text, h.names, h.lengths, h.size) == (g["text"], g["names"], g["lengths"], g["size"])
+    assert h.lines("@PG") == g["pg"]
+    assert list(cubam_b200.read_bam(GOLDEN / "empty.bam")) == []
+
+
+def test_bgzf_chunks_match_reference():
+    data = (GOLDEN / "text.raw").read_bytes()
+    for key, sizes in meta()["bgzf"].items():
+        name, chunk = key.split(":")
+        chunks = list(cubam_b200.inflate_chunks(GOLDEN / name, chunk_bytes=int(chunk), piece=int(chunk) // 3 + 1))
+        assert [int(c.numel()) for c in chunks] == sizes
+        assert b"".join(_np(c).tobytes() for c in chunks) == data
+        assert all(c.is_cuda for c in chunks)
+
+
+@pytest.mark.parametrize(
+    ("case", "file", "chunk"),
+    [
+        ("truncated", "truncated.gz", 8192),
+        ("bad_btype", "corrupt_bad_btype.gz", 8192),
+        ("bad_isize", "corrupt_bad_isize.gz", 8192),
+        ("isize_too_big", "corrupt_isize_too_big.gz", 8192),
+        ("bad_empty_member", "corrupt_bad_empty_member.gz", 8192),
+    ],
+)
+def test_bgzf_errors_match_reference(case, file, chunk):
+    kind, msg = meta()["errors"][case]
+    with pytest.raises(ValueError) as ei:
+        list(cubam_b200.inflate_chunks(GOLDEN / file, chunk_bytes=chunk))
+    assert kind == "ValueError" and str(ei.value) == msg
+
+
+def test_not_bgzf_empty_and_crc(tmp_path):
+    p = tmp_path / "n.gz"
+    p.write_bytes(b"hello world, not compressed" * 100)
+    with pytest.raises(ValueError, match=meta()["errors"]["not_bgzf"][1]):
+        list(cubam_b200.inflate_chunks(p, chunk_bytes=4096))
+    p.write_bytes(G.EOF_BLOCK)
+    assert sum(int(c.numel()) for c in cubam_b200.inflate_chunks(p, chunk_bytes=4096)) == 0
+    bad = GOLDEN / "corrupt_bad_crc.gz"
+    with pytest.raises(ValueError, match="CRC32"):
+        list(cubam_b200.inflate_chunks(bad, chunk_bytes=8192))
+    got = sum(int(c.numel()) for c in cubam_b200.inflate_chunks(bad, chunk_bytes=8192, check_crc=False))
+    assert got == 50_000
+
+
+def _payloads(seed: int):
+    """Member contents of many shapes: text, random, runs, BAM-like, empty, 1 byte, 65536 bytes."""
+    rng = random.Random(seed)
+    nrng = np.random.default_rng(seed)
+    out = [b"", b"x", b"\0" * 65536, bytes(nrng.integers(0, 256, 65536, dtype=np.uint8)), b"ab" * 32768]
+    for _ in range(40):
+        n = rng.choice([1, 2, 3, 100, 1000, 4095, 4096, 4097, 30000, 65280, 65535, 65536])
+        kind = rng.randrange(5)
+        if kind == 0:
+            words = [bytes(rng.choices(b"ACGT\t\n0123456789:chr", k=rng.randint(1, 12))) for _ in range(50)]
+            s = b"".join(rng.choice(words) for _ in range(n // 4 + 1))[:n]
+        elif kind == 1:
+            s = bytes(nrng.integers(0, 256, n, dtype=np.uint8))
+        elif kind == 2:
+            s = bytes(nrng.integers(0, 4, n, dtype=np.uint8) * 17)
+        elif kind == 3:
+            base = bytes(nrng.integers(0, 256, rng.randint(1, 40000), dtype=np.uint8))
+            s = (base * (n // max(len(base), 1) + 1))[:n]  # matches at long distances
+        else:
+            s = bytes(nrng.integers(2, 42, n, dtype=np.uint8))  # quality-like
+        out.append(s)
+    return out
+
+
+@pytest.mark.parametrize(
+    ("level", "strategy"),
+    [
+        (6, zlib.Z_DEFAULT_STRATEGY),
+        (1, zlib.Z_DEFAULT_STRATEGY),
+        (9, zlib.Z_DEFAULT_STRATEGY),
+        (0, zlib.Z_DEFAULT_STRATEGY),
+        (6, zlib.Z_FIXED),
+        (6, zlib.Z_HUFFMAN_ONLY),
+        (6, zlib.Z_RLE),
+        (6, zlib.Z_FILTERED),
+    ],
+)
+def test_inflate_matches_zlib(tmp_path, level, strategy):
+    payloads = _payloads(level * 10 + strategy)
+    raw = b"".join(member(p, level, strategy) for p in payloads)
+    buf = torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda()
+    jobs, s = G.scan_members(buf, True)
+    assert s.status == 0 and s.n_members == len(payloads)
+    assert s.total_out == sum(len(p) for p in payloads)
+    out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
+    summ = G.inflate_jobs(jobs, int(s.n_jobs), out, True)
+    G.check_inflate(summ)
+    assert _np(out).tobytes() == b"".join(payloads)
+
+
+def test_inflate_output_alignment_and_offsets():
+    """Members written at every output alignment (out_base offsets 0..17)."""
+    payloads = _payloads(3)[:12]
+    raw = b"".join(member(p) for p in payloads)
+    buf = torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda()
+    for shift in range(18):
+        jobs, s = G.scan_members(buf, True, out_base=shift)
+        out = torch.zeros(shift + int(s.total_out), dtype=torch.uint8, device="cuda")
+        G.check_inflate(G.inflate_jobs(jobs, int(s.n_jobs), out, True))
+        assert _np(out[shift:]).tobytes() == b"".join(payloads)
+        assert not bool(out[:shift].any())
+
+
+def test_inflate_corrupt_members_are_errors():
+    """Damaged members fail with the inflate or CRC status, never hang or overrun."""
+    rng = random.Random(7)
+    data = b"".join(bytes(rng.choices(b"ACGTN\t\n", k=200)) for _ in range(50))
+    good = member(data)
+    seen = set()
+    for trial in range(200):
+        m = bytearray(good)
+        for _ in range(rng.randint(1, 4)):
+            k = rng.randrange(18, len(m) - 8)
+            m[k] ^= 1 << rng.randrange(8)
+        buf = torch.frombuffer(bytearray(bytes(m) + G.EOF_BLOCK), dtype=torch.uint8).cuda()
+        jobs, s = G.scan_members(buf, True)
+        out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
+        st = int(G.read_struct(G.inflate_jobs(jobs, int(s.n_jobs), out, True), G._lib.InflateSummary).status)
+        d = zlib.decompressobj(-15)
+        try:
+            z = d.decompress(bytes(m[18:-8]), len(data) + 1)
+            zok = d.eof and len(z) == len(data)
+        except zlib.error:
+            zok = False
+        if not zok:
+            assert st in (G._lib.INFLATE, G._lib.CRC), trial
+        else:
+            assert st in (0, G._lib.CRC), trial
+            if st == 0:
+                assert _np(out).tobytes() == z
+        seen.add(st)
+    assert G._lib.INFLATE in seen
+
+
+def test_records_cross_members_and_chunks(tmp_path):
+    """The oracle's batches on a BAM with small members and chunks (records split across both)."""
+    raw = (GOLDEN / "mixed_b700.bam").read_bytes()
+    for chunk in (3000, 7777, 50_000):
+        exp = list(O.read_bam(raw, chunk, check_crc=True))
+        got = list(cubam_b200.read_bam(GOLDEN / "mixed_b700.bam", chunk_bytes=chunk, piece=1000))
+        assert [len(b) for b in got] == [len(b) for b in exp]
+        for g, e in zip(got, exp):
+            assert _np(g.data).tobytes() == e.data
+            assert _np(g.offset).tolist() == e.offset.tolist()
+            for k in O.FIELDS:
+                assert _np(getattr(g, k)).tolist() == e.columns[k].tolist()
