@@ -1,0 +1,467 @@
+"""Benchmark of the BAM reader hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config gex|small|atac]
+
+One step = one decode of the whole synthetic BAM of the workload (default: the
+GEX-shaped batch, 50,000,000 single-end 91 bp records over the 25 human
+chromosomes): BGZF member scan, inflate with CRC32/ISIZE checks, record chain,
+fixed columns and the CB/UB/GN tags.  The metric is GB/s of decompressed
+(uncompressed) BAM bytes, whole job over all ranks; records/s rides along.
+
+- ``value``: the batched decoder (``cubam_b200.batch``) with the compressed file
+  resident in HBM (one persistent inflate launch for all members), timed with
+  CUDA events between barriers, max over ranks.  Inputs (4-5 GB compressed,
+  12.6 GB inflated) are far larger than the 126 MB L2, so no flush is needed.
+- ``e2e``: the public API, ``cubam_b200.read_bam(path)`` from the page cache with
+  the CB/UB/GN tags decoded per batch: pread into pinned buffers, H2D copies, all
+  kernels, and a D2H read of the per-step checksum, timed by the device clock.
+- ``roofline``: the inflate kernel (the dominant one): decompressed bytes per
+  launch / its CUDA-event duration, against the measured HBM copy bandwidth.
+- ``cpu_baseline``: the C oracle (zlib inflate + record chain + columns, all host
+  cores) on a bounded prefix of the same file.
+- ``--impl reference``: cubam's reader needs CuPy, cuDF and nvCOMP and has no
+  CPU path; the reference arm times the CPU restatement of its reader path
+  (``oracle/cpu_decoder.c``, all host cores) on the same workload, rank 0 only.
+
+Multi-GPU (torchrun): every rank decodes its own copy of the file (replicas: the
+path shards by file with no exchange), ``scaling`` = weak.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BAM decode GB/s (uncompressed) & records/s on 1 B200"
+UNIT = "GB/s"
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="gex", choices=["gex", "small", "atac"])
+    ap.add_argument("--records", type=int, default=None, help="override the workload size (records)")
+    ap.add_argument("--chunk-bytes", type=int, default=256 << 20, help="compressed chunk of the e2e read_bam")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-mb", type=int, default=2048, help="compressed MB of the CPU baseline sample")
+    ap.add_argument("--workdir", default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM)), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+def workload(args):
+    from cubam_b200 import synth
+
+    cfg = synth.CONFIGS[args.config]
+    n = args.records or cfg.n_records
+    base = Path(args.workdir or ("/dev/shm" if Path("/dev/shm").exists() else "/tmp"))
+    path = base / f"cubam_bench_{cfg.name}_{n}_s{cfg.seed}.bam"
+    return cfg, n, path
+
+
+def ensure_file(args, rank, dist):
+    from cubam_b200 import synth
+
+    cfg, n, path = workload(args)
+    t = 0.0
+    if rank == 0 and not path.exists():
+        t0 = time.perf_counter()
+        tmp = path.with_suffix(f".tmp{os.getpid()}")
+        synth.write_bam(tmp, cfg, n_records=n)
+        tmp.replace(path)
+        t = time.perf_counter() - t0
+    if dist:
+        import torch.distributed as td
+
+        td.barrier()
+    return cfg, n, path, t
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(path: Path, sample_mb: int):
+    """The C oracle on the first ``sample_mb`` MB of compressed members, all host cores."""
+    import numpy as np
+
+    from oracle import cpu_oracle
+
+    raw = np.fromfile(path, dtype=np.uint8)
+    cores = os.cpu_count() or 1
+    cpu_oracle.decode_prefix(raw, sample_mb << 20, cores)  # warm-up: page faults of fresh buffers
+    d = min((cpu_oracle.decode_prefix(raw, sample_mb << 20, cores) for _ in range(2)), key=lambda x: x.seconds["total"])
+    secs = d.seconds["total"]
+    return {
+        "value": d.inflated_bytes / secs / 1e9,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "port",
+        "sample": f"first {d.n_members} members ({d.compressed_bytes / 1e6:.0f} MB compressed, "
+                  f"{d.inflated_bytes / 1e6:.0f} MB inflated, {len(d.offset)} records) of the same file: zlib "
+                  f"inflate + record chain + columns + CB/UB/GN tags in {secs:.2f} s",
+        "records_per_s": len(d.offset) / secs,
+    }
+
+
+def run_reference(args):
+    """CPU restatement of the reference's reader path (the reference has no CPU path of its own)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, n, path, gen_s = ensure_file(args, 0, None)
+    import numpy as np
+
+    from oracle import cpu_oracle
+
+    raw = np.fromfile(path, dtype=np.uint8)
+    cores = os.cpu_count() or 1
+    budget = args.cpu_sample_mb << 20
+    for _ in range(args.warmup):
+        cpu_oracle.decode_prefix(raw, min(budget, 64 << 20), cores)
+    times, inflated, recs, members, comp = [], 0, 0, 0, 0
+    for _ in range(args.steps):
+        d = cpu_oracle.decode_prefix(raw, budget, cores)
+        times.append(d.seconds["total"])
+        inflated, recs, members, comp = d.inflated_bytes, len(d.offset), d.n_members, d.compressed_bytes
+    ms = statistics.mean(times) * 1e3
+    value = inflated / (ms / 1e3) / 1e9
+    sample = (f"first {members} members ({comp / 1e6:.0f} MB compressed, {inflated / 1e6:.0f} MB inflated, "
+              f"{recs} records) of the {cfg.name} workload per step")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{cfg.name}: {n} records, zlib level {cfg.level}, seed {cfg.seed}",
+                   "records_per_step": recs},
+        "records_per_s": recs / (ms / 1e3),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    dist = int(os.environ.get("WORLD_SIZE", "1")) > 1
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    if dist:
+        import datetime
+
+        import torch.distributed as td
+
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    cfg, n, path, gen_s = ensure_file(args, rank, dist)
+
+    import cubam_b200
+    from cubam_b200 import batch
+
+    header = cubam_b200.BamHeader.read(path)
+    comp = batch.load_compressed(path)
+    torch.cuda.synchronize()
+    counter = {}
+    tags = ("CB", "UB", "GN")
+
+    def step(ev=None, cnt=None):
+        return batch.decode_resident(comp, header, tags=tags, events=ev, counter=cnt)
+
+    for _ in range(max(args.warmup, 0)):
+        res = step()
+        del res
+    torch.cuda.synchronize()
+    res = step()
+    inflated = res.inflated_bytes
+    n_rec = len(res)
+    n_members = res.n_members
+    del res
+
+    def barrier():
+        if dist:
+            import torch.distributed as td
+
+            td.barrier()
+
+    evs = []
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(args.steps):
+            ev = batch.StageEvents()
+            r = step(ev, counter)
+            evs.append(ev)
+            del r
+        stop.record()
+        torch.cuda.synchronize()
+        barrier()
+    ms = start.elapsed_time(stop) / args.steps
+    if dist:
+        import torch.distributed as td
+
+        t = torch.tensor([ms], device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        ms = float(t.item())
+    stage = {k: statistics.mean(e.ms()[k] for e in evs) for k in evs[0].ms()}
+    inflate_ms = stage["inflated"]
+    value = inflated * world / (ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    achieved = inflated / (inflate_ms / 1e3) / 1e9
+
+    # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)
+    plain = None
+    if not args.no_plain:
+        plain = plain_per_chunk(comp, header, args.chunk_bytes, tags)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(path, args, tags, inflated, rank, dist)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(path, args.cpu_sample_mb)
+    if rank != 0:
+        if dist:
+            import torch.distributed as td
+
+            td.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {
+            "workload": f"{cfg.name}: {n} records, zlib level {cfg.level}, seed {cfg.seed}",
+            "compressed_bytes": int(comp.numel()),
+            "inflated_bytes": inflated,
+            "members": n_members,
+            "records": n_rec,
+            "tags": list(tags),
+            "form": "batched: whole file resident, one persistent inflate launch",
+            "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}",
+            "generate_s": round(gen_s, 1),
+        },
+        "records_per_s": n_rec * world / (ms / 1e3),
+        "stages_ms": {k: round(v, 3) for k, v in stage.items()},
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "k_inflate",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_kind": peak_kind,
+            "algorithmic": "decompressed bytes (sum of ISIZE) per launch",
+            "traffic": None,
+        },
+        "clocks": clk.summary(),
+        "gpu_launches": counter.get("launches", 0),
+    }
+    if plain:
+        line["plain_per_chunk"] = plain
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    if dist:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+
+
+def plain_per_chunk(comp, header, chunk_bytes, tags):
+    """One pass of the per-chunk form (scan, sync, inflate, chain, sync, decode per chunk) on resident chunks."""
+    import torch
+
+    from cubam_b200 import _lib
+    from cubam_b200.bam import RecordBatch, record_chain
+    from cubam_b200.bgzf import _inflate_blocks, check_inflate, raise_status, read_struct
+
+    def one_pass():
+        n = int(comp.numel())
+        carry_c = torch.empty(0, dtype=torch.uint8, device="cuda")
+        carry_r = torch.empty(0, dtype=torch.uint8, device="cuda")
+        skip = header.size
+        recs = 0
+        for a in range(0, n, chunk_bytes):
+            b = min(a + chunk_bytes, n)
+            buf = torch.cat([carry_c, comp[a:b]]) if carry_c.numel() else comp[a:b]
+            data, used, summ = _inflate_blocks(buf, b >= n, carry_r, True, True)
+            carry_c = buf[used:].clone()
+            if skip:
+                k = min(skip, int(data.numel()))
+                data = data[k:]
+                skip -= k
+            if int(data.numel()) == 0:
+                carry_r = data
+                continue
+            offsets, cs = record_chain(data, len(header.names))
+            if summ is not None:
+                check_inflate(summ)
+            s = read_struct(cs, _lib.ChainSummary)
+            raise_status(s.status, "record chain")
+            off = offsets[: s.n_records]
+            carry_r = data[s.tail:].clone()
+            if off.numel():
+                bt = RecordBatch.decode(data, off, header)
+                bt.tags(*tags)
+                recs += len(bt)
+        return recs
+
+    one_pass()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    recs = one_pass()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    return {"ms_per_step": ms, "records": recs, "chunk_bytes": chunk_bytes}
+
+
+def run_e2e(path, args, tags, inflated, rank, dist):
+    """read_bam through the public API, file -> pinned -> device, with a D2H checksum per step."""
+    import torch
+
+    import cubam_b200
+
+    size = os.path.getsize(path)
+
+    def one():
+        chk = torch.zeros(1, dtype=torch.int64, device="cuda")
+        recs = 0
+        for b in cubam_b200.read_bam(path, chunk_bytes=args.chunk_bytes):
+            for t in b.tags(*tags):
+                chk += t.length.sum()
+            chk += b.pos.sum()
+            recs += len(b)
+        return recs, int(chk.item())  # the D2H read of the step's result
+
+    one()
+    torch.cuda.synchronize()
+    if dist:
+        import torch.distributed as td
+
+        td.barrier()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    s.record()
+    for _ in range(args.e2e_steps):
+        recs, _ = one()
+    e.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.e2e_steps
+    ms = s.elapsed_time(e) / args.e2e_steps
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if dist:
+        import torch.distributed as td
+
+        t = torch.tensor([ms], device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        ms = float(t.item())
+    return {
+        "value": inflated * world / (ms / 1e3) / 1e9,
+        "unit": UNIT,
+        "h2d_bytes_per_step": size,
+        "d2h_bytes_per_step": 8,
+        "ms_per_step": ms,
+        "wall_ms_per_step": wall * 1e3,
+        "records_per_s": recs * world / (ms / 1e3),
+        "chunk_bytes": args.chunk_bytes,
+        "api": "cubam_b200.read_bam(path) + RecordBatch.tags('CB','UB','GN')",
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -50,6 +50,15 @@ _TYPES = {
 }
 
 
+_SIGNED_VIEW = {torch.uint16: torch.int16, torch.uint32: torch.int32, torch.uint64: torch.int64}
+
+
+def _index(t: torch.Tensor, idx: torch.Tensor) -> torch.Tensor:
+    """``t[idx]`` for every dtype (unsigned 16/32/64-bit tensors go through same-width signed views)."""
+    s = _SIGNED_VIEW.get(t.dtype)
+    return t[idx] if s is None else t.view(s)[idx].view(t.dtype)
+
+
 def _ptr(t: torch.Tensor | None):
     return None if t is None or t.numel() == 0 else t.data_ptr()
 
@@ -294,7 +303,7 @@ class RecordBatch:
         idx = torch.as_tensor(idx, device="cuda")
         if idx.dtype == torch.bool:
             idx = torch.nonzero(idx).flatten()
-        return RecordBatch(self.data, self.offset[idx], self.header, {k: v[idx] for k, v in self.columns.items()})
+        return RecordBatch(self.data, self.offset[idx], self.header, {k: _index(v, idx) for k, v in self.columns.items()})
 
     def record_sizes(self) -> torch.Tensor:
         """Bytes of each record, its length field included (int64)."""

@@ -24,6 +24,22 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared"]
 
 
+SYNTH_SRC = CSRC / "host" / "synth.c"
+SYNTH_LIB = OUT_DIR / "libcubam_synth.so"
+
+
+def build_synth(force: bool = False) -> Path:
+    """The host library of the synthetic BAM generator (gcc, zlib, pthreads)."""
+    if not force and SYNTH_LIB.exists() and SYNTH_LIB.stat().st_mtime > SYNTH_SRC.stat().st_mtime:
+        return SYNTH_LIB
+    OUT_DIR.mkdir(exist_ok=True)
+    tmp = OUT_DIR / f".libcubam_synth.{os.getpid()}.so"
+    cmd = ["gcc", "-O3", "-shared", "-fPIC", "-pthread", str(SYNTH_SRC), "-o", str(tmp), "-lz", "-lm"]
+    subprocess.run(cmd, check=True)
+    tmp.replace(SYNTH_LIB)
+    return SYNTH_LIB
+
+
 def _sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [HEADER]
 
@@ -66,3 +82,4 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_synth(force="--force" in sys.argv))

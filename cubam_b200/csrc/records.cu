@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(FIN_NT) k_rec_finish(const uint8_t* buf, int64
         __syncthreads();
     }
     __shared__ long long s_last;
-    if (tid == 0) s_last = -1;
+    if (tid == 0) s_last = 0;  // raised with an unsigned atomicMax; candidate 0 is always on the chain
     __syncthreads();
     if (last >= 0) atomicMax(reinterpret_cast<unsigned long long*>(&s_last), (unsigned long long)last);
     __syncthreads();

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(FIN_NT) k_scan_finish(const uint8_t* buf, long
     const int tid = threadIdx.x;
     if (tid == 0) {
         s_breaks = 0;
-        s_last = -1;
+        s_last = 0;  // raised with an unsigned atomicMax below; candidate 0 is always kept
         summary->n_members = 0;
         summary->n_jobs = 0;
         summary->used = 0;
