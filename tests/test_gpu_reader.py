@@ -30,6 +30,8 @@ def _np(t):
 
 
 def member(data: bytes, level: int = 6, strategy: int = zlib.Z_DEFAULT_STRATEGY, mem_level: int = 8) -> bytes:
+    if not data:  # the reference accepts an empty member only in the exact form of the EOF member
+        return G.EOF_BLOCK
     c = zlib.compressobj(level, zlib.DEFLATED, -15, mem_level, strategy)
     payload = c.compress(data) + c.flush()
     if len(payload) + 26 > 65536:  # does not shrink enough: a stored member, as BGZF writers do
