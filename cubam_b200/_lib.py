@@ -67,6 +67,7 @@ _SIGNATURES = {
     "cb_device_sm_count": (c_int, []),
     "cb_scan_workspace_bytes": (c_size_t, [I64]),
     "cb_scan_members": (c_int, [P, I64, c_int, I64, P, I64, P, P, c_size_t, P]),
+    "cb_scan_members_noalloc": (c_int, [P, I64, c_int, I64, P, I64, P, P]),
     "cb_inflate_workspace_bytes": (c_size_t, []),
     "cb_inflate": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, P]),
     "cb_record_chain_workspace_bytes": (c_size_t, [I64]),

@@ -13,6 +13,11 @@ int cb_set_error(cudaError_t e) {
     return CB_ERR_CUDA;
 }
 
+int cb_set_error_text(int code, const char* text) {
+    std::snprintf(g_err, sizeof(g_err), "%s", text);
+    return code;
+}
+
 extern "C" const char* cb_version(void) { return "cubam_b200 0.1.0 (sm_100a)"; }
 
 extern "C" const char* cb_last_error(void) { return g_err; }

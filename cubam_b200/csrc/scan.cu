@@ -310,3 +310,46 @@ extern "C" int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t o
     scan::k_scan_finish<<<1, scan::FIN_NT, 0, s>>>(buf, n, eof, out_base_off, jobs, cap, summary, w);
     return cb_set_error(cudaGetLastError());
 }
+
+// ---------------------------------------------------------------- the scan without allocation
+// cb_scan_members with its scratch in a file-scope device array (see the header): the array holds
+// the workspace of an input of CB_NOALLOC_SCAN_MAX_BYTES bytes, laid out as scan::carve lays out a
+// caller's workspace.
+
+namespace cb {
+namespace scan {
+
+constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr long long NOALLOC_TILES = (CB_NOALLOC_SCAN_MAX_BYTES + 15 + 16) / 16 / NT + 2;
+constexpr long long NOALLOC_CAP = CB_NOALLOC_SCAN_MAX_BYTES / 28 + 1024;
+constexpr size_t NOALLOC_SCRATCH_BYTES =
+    256 + a256(NOALLOC_TILES * 4) + a256(NOALLOC_TILES * 8) + a256(NOALLOC_CAP * 8) + a256(NOALLOC_CAP) + 256;
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+static void* g_noalloc_ptr[64];  // the array's device address, per device, looked up on first use
+
+}  // namespace scan
+}  // namespace cb
+
+int cb_set_error_text(int code, const char* text);  // abi.cu
+
+extern "C" int cb_scan_members_noalloc(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off,
+                                       cb_member_job* jobs, int64_t cap, cb_scan_summary* summary, void* stream) {
+    if (n < 0) return CB_ERR_ARG;
+    if (n > CB_NOALLOC_SCAN_MAX_BYTES || scan::ws_bytes(n) > scan::NOALLOC_SCRATCH_BYTES)
+        return cb_set_error_text(CB_ERR_CAPACITY,
+                                 "cb_scan_members_noalloc: input larger than its fixed scratch (16 MiB at most)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cb_set_error(e);
+    if (dev < 0 || dev >= 64) return cb_set_error_text(CB_ERR_ARG, "cb_scan_members_noalloc: device index >= 64");
+    if (!scan::g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, scan::g_noalloc_scratch);
+        if (e != cudaSuccess) return cb_set_error(e);
+        scan::g_noalloc_ptr[dev] = p;
+    }
+    return cb_scan_members(buf, n, eof, out_base_off, jobs, cap, summary, scan::g_noalloc_ptr[dev],
+                           scan::NOALLOC_SCRATCH_BYTES, stream);
+}

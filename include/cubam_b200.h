@@ -97,6 +97,23 @@ size_t cb_scan_workspace_bytes(int64_t n);
 int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off, cb_member_job* jobs, int64_t cap,
                     cb_scan_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- Member scan that allocates nothing (no counterpart in the reference) ----------------------
+ * Some callers cannot allocate device memory for a workspace: a serving process whose device memory
+ * is owned up front by one pool (RMM, PyTorch's caching allocator) that must not see cudaMalloc
+ * behind its back, a caller from another runtime (cgo, JNI) with no device allocator of its own, or
+ * a latency-sensitive loop where cudaMalloc/cudaFree would synchronise the device.  This entry point
+ * is cb_scan_members with its scratch in a fixed array inside the library instead of a workspace:
+ * inputs of at most CB_NOALLOC_SCAN_MAX_BYTES (16 MiB) bytes, about 5.5 MB of scratch that every GPU
+ * which loads the library holds until the process exits; larger inputs get CB_ERR_CAPACITY (and
+ * cb_last_error() says why) before anything is launched.  The caller still passes the input, the
+ * job table and the summary.  The first call on a device looks the array's address up for that
+ * device (cudaGetSymbolAddress), so make the first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other threads) race on it and must
+ * be serialised by the caller; nothing in it needs to start at zero. */
+#define CB_NOALLOC_SCAN_MAX_BYTES (16LL << 20)
+int cb_scan_members_noalloc(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off, cb_member_job* jobs,
+                            int64_t cap, cb_scan_summary* summary, void* stream);
+
 /* ---- Inflate: replaces nvcompBatchedDeflateDecompressAsync and the status/size check
  *      (src/cubam/bgzf.py:587-611); adds the CRC32 check ---------------------------------------- */
 
