@@ -390,7 +390,7 @@ class RecordBatch:
 def record_chain(data: torch.Tensor, n_ref: int):
     """Launch ``cb_record_chain``; returns ``(offsets capacity buffer, device summary)`` without a sync."""
     n = int(data.numel())
-    cap = n // 32 + 1024
+    cap = n // 37 + 2  # records are at least 37 bytes
     offsets = torch.empty(cap, dtype=torch.int64, device="cuda")
     summ = torch.zeros(ctypes_sizeof(_lib.ChainSummary), dtype=torch.uint8, device="cuda")
     ws = torch.empty(max(int(_lib.lib.cb_record_chain_workspace_bytes(n)), 256), dtype=torch.uint8, device="cuda")

@@ -150,7 +150,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
         data = out[base + header.size : base + int(info.total_out)]
         base += int(info.total_out)
         n = int(data.numel())
-        cap = n // 32 + 1024
+        cap = n // 37 + 2  # records are at least 37 bytes
         offsets = torch.empty(cap, dtype=torch.int64, device="cuda")
         csumm = torch.zeros(ctypes_sizeof(_lib.ChainSummary), dtype=torch.uint8, device="cuda")
         ws = torch.empty(max(int(_lib.lib.cb_record_chain_workspace_bytes(n)), 256), dtype=torch.uint8,

@@ -1,0 +1,299 @@
+// The record chain of an inflated chunk on B200: replaces record_candidates + record_ends + chain
+// (src/cubam/_kernels.py:250-289, src/cubam/_kernels.py:676-702, src/cubam/bam.py:403-418).
+//
+// cubam tests the record predicate (is_record, src/cubam/_kernels.py:250-278) at every byte offset and
+// keeps the chain from offset 0.  Only offsets on that chain matter: the result is the walk from 0 that
+// follows block_size while the predicate holds, which is O(records), not O(bytes).  It is walked in
+// parallel by tiles:
+//
+//  1. k_walk: one thread per 2 KB tile finds the tile's first offset that passes the predicate and
+//     walks the block_size links from it (each record checked with the full predicate) up to the first
+//     offset past the tile: first[t], count[t], exit[t], and whether the walk broke inside the tile.
+//  2. k_check: tile t's walk is the true chain when its first offset is where the previous non-empty
+//     tile's walk left (exit); a tile whose candidate is not on the chain (a spurious match of the
+//     predicate) makes the chunk take the serial path.  With none (the usual case, none were seen in
+//     hundreds of MB of BAM data), the chain is the union of the tile walks up to the first broken one.
+//  3. k_count_* : prefix sum of the tile counts (three kernels), then k_emit re-walks each tile to
+//     write its offsets; k_finish writes the summary (records, tail, errors).
+//  4. k_serial: the chain walked by one thread, for chunks where the tile walks disagree.
+
+#include "common.cuh"
+
+namespace cb {
+namespace chain {
+
+constexpr long long T = 2048;   // bytes per tile
+constexpr int NT = 256;
+constexpr int SCAN = 1024;       // tiles per block of the count scan
+
+struct Ws {
+    int64_t* first;    // per tile
+    int64_t* exit;
+    int32_t* count;    // records; bit 31: the walk broke inside the tile
+    int64_t* base;     // exclusive prefix of the counts
+    int64_t* bsum;     // per scan block
+    int64_t* meta;     // [0] inconsistent tile (min) [1] first broken tile (min) [2] any candidate [3] total
+    long long ntiles, nblocks;
+};
+
+__host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+__host__ __device__ inline Ws carve(void* ws, long long n) {
+    Ws w;
+    w.ntiles = (n + T - 1) / T;
+    if (w.ntiles < 1) w.ntiles = 1;
+    w.nblocks = (w.ntiles + SCAN - 1) / SCAN;
+    uint8_t* p = reinterpret_cast<uint8_t*>(ws);
+    w.meta = reinterpret_cast<int64_t*>(p);
+    p += 256;
+    w.first = reinterpret_cast<int64_t*>(p);
+    p += align256(w.ntiles * 8);
+    w.exit = reinterpret_cast<int64_t*>(p);
+    p += align256(w.ntiles * 8);
+    w.count = reinterpret_cast<int32_t*>(p);
+    p += align256(w.ntiles * 4);
+    w.base = reinterpret_cast<int64_t*>(p);
+    p += align256(w.ntiles * 8);
+    w.bsum = reinterpret_cast<int64_t*>(p);
+    return w;
+}
+
+__host__ inline size_t ws_bytes(long long n) {
+    long long ntiles = (n + T - 1) / T;
+    if (ntiles < 1) ntiles = 1;
+    long long nblocks = (ntiles + SCAN - 1) / SCAN;
+    return 256 + 3 * align256(ntiles * 8) + align256(ntiles * 4) + align256(nblocks * 8) + 256;
+}
+
+__device__ __forceinline__ int reg2bin(int beg, int end) {
+    --end;
+    if (beg >> 14 == end >> 14) return 4681 + (beg >> 14);
+    if (beg >> 17 == end >> 17) return 585 + (beg >> 17);
+    if (beg >> 20 == end >> 20) return 73 + (beg >> 20);
+    if (beg >> 23 == end >> 23) return 9 + (beg >> 23);
+    if (beg >> 26 == end >> 26) return 1 + (beg >> 26);
+    return 0;
+}
+
+// The reference's record predicate at offset o (src/cubam/_kernels.py:250-278).
+__device__ bool is_record(const uint8_t* b, long long n, long long o, int n_ref) {
+    if (o < 0 || o + 36 > n) return false;
+    const int bs = (int)ld_u32(b, o);
+    if (bs < 33 || bs > (1 << 22) || o + 4 + (long long)bs > n) return false;
+    const int ref = (int)ld_u32(b, o + 4), pos = (int)ld_u32(b, o + 8);
+    const int nref = (int)ld_u32(b, o + 24), npos = (int)ld_u32(b, o + 28);
+    if (ref < -1 || ref >= n_ref || pos < -1 || nref < -1 || nref >= n_ref || npos < -1) return false;
+    const uint32_t lrn = b[o + 12], ncig = ld_u16(b, o + 16), flag = ld_u16(b, o + 18), lseq = ld_u32(b, o + 20);
+    if (lrn < 2 || flag >= 4096 || lseq > (1u << 22)) return false;
+    if (32LL + lrn + 4LL * ncig + (lseq + 1) / 2 + lseq > (long long)bs) return false;
+    const long long nm = o + 36;
+    if (b[nm + lrn - 1] != 0) return false;
+    for (uint32_t i = 0; i + 1 < lrn; i++) {
+        const uint8_t c = b[nm + i];
+        if (c < 33 || c > 126 || c == '@') return false;
+    }
+    const long long cg = nm + lrn;
+    long long rlen = 0;
+    for (uint32_t i = 0; i < ncig; i++) {
+        const uint32_t v = ld_u32(b, cg + 4LL * i), op = v & 15;
+        if (op > 8) return false;
+        if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) rlen += v >> 4;
+    }
+    if (pos >= 0) {
+        const int end = pos + (int)(rlen > 0 ? rlen : 1);
+        if (ld_u16(b, o + 14) != (uint32_t)reg2bin(pos, end)) return false;
+    }
+    return true;
+}
+
+// First offset in [lo, hi) that passes the predicate, or -1.  block_size is read from aligned words
+// (a 64-bit window) so that most offsets are rejected without the full test.
+__device__ long long first_candidate(const uint8_t* b, long long n, long long lo, long long hi, int n_ref) {
+    for (long long o = lo; o < hi; o++) {
+        if (o + 4 > n) return -1;
+        const uint32_t bs = ld_u32(b, o);
+        if (bs - 33u > (1u << 22) - 33u) continue;
+        if (is_record(b, n, o, n_ref)) return o;
+    }
+    return -1;
+}
+
+__global__ void k_init(Ws w) {
+    w.meta[0] = INT64_MAX;
+    w.meta[1] = INT64_MAX;
+    w.meta[2] = 0;
+    w.meta[3] = 0;
+}
+
+__global__ void __launch_bounds__(NT) k_walk(const uint8_t* b, long long n, int n_ref, Ws w) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long ts = t * T, te = min(ts + T, n);
+        const long long c = first_candidate(b, n, ts, te, n_ref);
+        long long o = c;
+        int cnt = 0;
+        bool broken = false;
+        if (c >= 0) {
+            atomicOr(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
+            while (o < te) {
+                if (!is_record(b, n, o, n_ref)) {
+                    broken = true;
+                    break;
+                }
+                cnt++;
+                o += 4 + (long long)ld_u32(b, o);
+            }
+            if (broken) atomicMin(reinterpret_cast<long long*>(&w.meta[1]), t);
+        }
+        w.first[t] = c;
+        w.exit[t] = c >= 0 ? o : -1;
+        w.count[t] = cnt | (broken ? (int)0x80000000 : 0);
+    }
+}
+
+// Is each non-empty tile entered by the chain at its first candidate?
+__global__ void __launch_bounds__(NT) k_check(Ws w) {
+    const long long end = w.meta[1];  // the chain ends in this tile (if any)
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long f = w.first[t];
+        if (f < 0 || t > end) continue;
+        long long entry = 0;
+        for (long long u = t - 1; u >= 0; u--) {
+            if (w.first[u] >= 0) {
+                entry = w.exit[u];
+                break;
+            }
+        }
+        if (entry != f) atomicMin(reinterpret_cast<long long*>(&w.meta[0]), t);
+    }
+}
+
+// Prefix sum of the tile counts (tiles after the end of the chain count 0).
+__global__ void __launch_bounds__(SCAN) k_count_blocks(Ws w) {
+    __shared__ int64_t sm[33];
+    const long long end = w.meta[1];
+    const long long t = (long long)blockIdx.x * SCAN + threadIdx.x;
+    int64_t v = (t < w.ntiles && t <= end) ? (int64_t)(w.count[t] & 0x7fffffff) : 0;
+    int64_t tot;
+    const int64_t x = block_exclusive_scan<SCAN>(v, tot, sm);
+    if (t < w.ntiles) w.base[t] = x;
+    if (threadIdx.x == 0) w.bsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN) k_count_top(Ws w) {
+    __shared__ int64_t sm[33];
+    int64_t carry = 0;
+    for (long long b0 = 0; b0 < w.nblocks; b0 += SCAN) {
+        const long long i = b0 + threadIdx.x;
+        const int64_t v = i < w.nblocks ? w.bsum[i] : 0;
+        int64_t tot;
+        const int64_t x = block_exclusive_scan<SCAN>(v, tot, sm);
+        if (i < w.nblocks) w.bsum[i] = carry + x;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) w.meta[3] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN) k_count_add(Ws w) {
+    const long long t = (long long)blockIdx.x * SCAN + threadIdx.x;
+    if (t < w.ntiles) w.base[t] += w.bsum[blockIdx.x];
+}
+
+__global__ void __launch_bounds__(NT) k_emit(const uint8_t* b, long long n, Ws w, int64_t* out, long long cap) {
+    if (w.meta[0] != INT64_MAX || w.meta[3] > cap) return;
+    const long long end = w.meta[1];
+    if (w.first[0] != 0) return;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t > end) continue;
+        const int cnt = w.count[t] & 0x7fffffff;
+        long long o = w.first[t];
+        long long k = w.base[t];
+        for (int i = 0; i < cnt; i++) {
+            out[k + i] = o;
+            o += 4 + (long long)ld_u32(b, o);
+        }
+    }
+}
+
+// The chain walked by one thread (tiles that disagree).
+__global__ void k_serial(const uint8_t* b, long long n, int n_ref, Ws w, int64_t* out, long long cap,
+                         cb_chain_summary* summary) {
+    if (w.meta[0] == INT64_MAX || w.first[0] != 0) return;
+    long long o = 0, k = 0;
+    while (is_record(b, n, o, n_ref)) {
+        if (k < cap) out[k] = o;
+        k++;
+        o += 4 + (long long)ld_u32(b, o);
+    }
+    summary->n_records = k;
+    summary->tail = o;
+    summary->n_candidates = -1;
+    summary->chained = 0;
+    summary->status = k > cap ? CB_ERR_CAPACITY : CB_OK;
+}
+
+__global__ void k_finish(long long n, Ws w, long long cap, cb_chain_summary* summary) {
+    if (n == 0 || w.meta[2] == 0) {  // no record candidate anywhere: nothing on the chain, carry all
+        summary->n_records = 0;
+        summary->tail = 0;
+        summary->n_candidates = 0;
+        summary->chained = 1;
+        summary->status = CB_OK;
+        return;
+    }
+    if (w.first[0] != 0) {  // offset 0 is not a record while another offset is
+        summary->n_records = 0;
+        summary->tail = 0;
+        summary->n_candidates = -1;
+        summary->chained = 1;
+        summary->status = CB_ERR_NO_CHAIN;
+        return;
+    }
+    if (w.meta[0] != INT64_MAX) return;  // k_serial writes the summary
+    const long long end = w.meta[1];
+    long long last = end;
+    if (last == INT64_MAX) {  // the chain runs to the end of the data: its last non-empty tile
+        last = w.ntiles - 1;
+        while (last > 0 && w.first[last] < 0) last--;
+    }
+    summary->n_records = w.meta[3];
+    summary->tail = w.exit[last];
+    summary->n_candidates = -1;
+    summary->chained = 1;
+    summary->status = w.meta[3] > cap ? CB_ERR_CAPACITY : CB_OK;
+}
+
+}  // namespace chain
+}  // namespace cb
+
+using namespace cb;
+
+int cb_set_error(cudaError_t e);  // abi.cu
+
+extern "C" size_t cb_record_chain_workspace_bytes(int64_t n) { return chain::ws_bytes(n < 0 ? 0 : n); }
+
+extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, int64_t* offsets, int64_t cap,
+                               cb_chain_summary* summary, void* workspace, size_t workspace_bytes, void* stream) {
+    if (n < 0 || !summary || !workspace || (n > 0 && (!data || !offsets)) || cap < 0) return CB_ERR_ARG;
+    if (workspace_bytes < chain::ws_bytes(n)) return CB_ERR_CAPACITY;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    chain::Ws w = chain::carve(workspace, n);
+    const long long sms = cb_device_sm_count();
+    long long grid = (w.ntiles + chain::NT - 1) / chain::NT;
+    if (grid > sms * 16) grid = sms * 16;
+    if (grid < 1) grid = 1;
+    chain::k_init<<<1, 1, 0, s>>>(w);
+    if (n > 0) {
+        chain::k_walk<<<(unsigned)grid, chain::NT, 0, s>>>(data, n, n_ref, w);
+        chain::k_check<<<(unsigned)grid, chain::NT, 0, s>>>(w);
+        chain::k_count_blocks<<<(unsigned)w.nblocks, chain::SCAN, 0, s>>>(w);
+        chain::k_count_top<<<1, chain::SCAN, 0, s>>>(w);
+        chain::k_count_add<<<(unsigned)w.nblocks, chain::SCAN, 0, s>>>(w);
+        chain::k_emit<<<(unsigned)grid, chain::NT, 0, s>>>(data, n, w, offsets, cap);
+        chain::k_serial<<<1, 1, 0, s>>>(data, n, n_ref, w, offsets, cap, summary);
+    }
+    chain::k_finish<<<1, 1, 0, s>>>(n, w, cap, summary);
+    return cb_set_error(cudaGetLastError());
+}

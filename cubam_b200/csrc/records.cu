@@ -1,322 +1,14 @@
-// BAM records on B200: the record chain (src/cubam/_kernels.py:250-289, src/cubam/bam.py:403-418),
-// the fixed columns (src/cubam/_kernels.py:292-319), the aux tags (src/cubam/_kernels.py:334-388) and
-// the on-request decoders (src/cubam/_kernels.py:322-620, src/cubam/bam.py:299-400).
-//
-// Record chain:
-//  1. k_rec_count: every byte offset of the inflated chunk is tested with the reference's record
-//     predicate.  Each thread loads 16 bytes with one 128-bit load plus the next 4 bytes of its
-//     neighbour, so the block_size window of all 16 offsets is in registers; most offsets fail the
-//     33 <= block_size <= 2^22 test there.  Survivors get the full predicate.  Counts per 4 KB tile.
-//  2. k_rec_tiles: prefix sum of the tile counts (one block).
-//  3. k_rec_write: the candidates, in order, straight into the caller's offset array.
-//  4. k_rec_links: does each candidate end where the next starts (grid)?
-//  5. k_rec_finish: one block: in the usual case the candidates are the records; otherwise the
-//     reference's pointer jumping from offset 0 runs in this block and the chain is compacted in place.
+// BAM record columns on B200: the fixed columns (src/cubam/_kernels.py:292-319), the aux tags
+// (src/cubam/_kernels.py:334-388) and the on-request decoders (src/cubam/_kernels.py:322-620,
+// src/cubam/bam.py:299-400).  The record chain itself is in chain.cu.
 
 #include "common.cuh"
 
 namespace cb {
 namespace rec {
 
-constexpr int NT = 256;
-constexpr int TILE = NT * 16;
-constexpr int FIN_NT = 1024;
-
-struct Ws {
-    uint32_t* tile_count;
-    int64_t* tile_off;
-    int64_t* meta;     // [0] candidates, [1] status, [2] breaks
-    int64_t* jump;     // pointer jumping (slow path)
-    int64_t* jump2;
-    uint8_t* mark;
-    long long ntiles, cap;
-};
-
-__host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-
-__host__ __device__ inline long long n_tiles(const uint8_t* buf, long long n) {
-    uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
-    long long chunks = (long long)(((uintptr_t)buf + n + 15 - base) >> 4);
-    return (chunks + NT - 1) / NT + 1;
-}
-
-__host__ __device__ inline long long too_many(long long n) { return n / 32 + 1024; }
-
-__host__ __device__ inline Ws carve(void* ws, const uint8_t* buf, long long n) {
-    Ws w;
-    w.ntiles = n_tiles(buf, n);
-    w.cap = too_many(n);
-    uint8_t* p = reinterpret_cast<uint8_t*>(ws);
-    w.meta = reinterpret_cast<int64_t*>(p);
-    p += 256;
-    w.tile_count = reinterpret_cast<uint32_t*>(p);
-    p += align256(w.ntiles * 4);
-    w.tile_off = reinterpret_cast<int64_t*>(p);
-    p += align256(w.ntiles * 8);
-    w.jump = reinterpret_cast<int64_t*>(p);
-    p += align256((w.cap + 1) * 8);
-    w.jump2 = reinterpret_cast<int64_t*>(p);
-    p += align256((w.cap + 1) * 8);
-    w.mark = p;
-    return w;
-}
-
-__host__ inline size_t ws_bytes(long long n) {
-    long long ntiles = (n + 32) / 16 / NT + 2;
-    long long cap = too_many(n);
-    return 256 + align256(ntiles * 4) + align256(ntiles * 8) + 2 * align256((cap + 1) * 8) + align256(cap + 1) + 256;
-}
-
-__device__ __forceinline__ int reg2bin(int beg, int end) {
-    --end;
-    if (beg >> 14 == end >> 14) return 4681 + (beg >> 14);
-    if (beg >> 17 == end >> 17) return 585 + (beg >> 17);
-    if (beg >> 20 == end >> 20) return 73 + (beg >> 20);
-    if (beg >> 23 == end >> 23) return 9 + (beg >> 23);
-    if (beg >> 26 == end >> 26) return 1 + (beg >> 26);
-    return 0;
-}
-
 __device__ __forceinline__ bool ref_consuming(uint32_t op) {
     return op == 0 || op == 2 || op == 3 || op == 7 || op == 8;  // M D N = X
-}
-
-// The reference's record predicate (src/cubam/_kernels.py:250-278), after block_size `bs`
-// (read by the caller) passed 33 <= bs <= 2^22.
-__device__ bool record_rest(const uint8_t* b, long long n, long long o, int bs, int n_ref) {
-    if (o + 36 > n || o + 4 + (long long)bs > n) return false;
-    int ref = (int)ld_u32(b, o + 4), pos = (int)ld_u32(b, o + 8);
-    int nref = (int)ld_u32(b, o + 24), npos = (int)ld_u32(b, o + 28);
-    if (ref < -1 || ref >= n_ref || pos < -1 || nref < -1 || nref >= n_ref || npos < -1) return false;
-    uint32_t lrn = b[o + 12], ncig = ld_u16(b, o + 16), flag = ld_u16(b, o + 18), lseq = ld_u32(b, o + 20);
-    if (lrn < 2 || flag >= 4096 || lseq > (1u << 22)) return false;
-    if (32LL + lrn + 4LL * ncig + (lseq + 1) / 2 + lseq > (long long)bs) return false;
-    const long long nm = o + 36;
-    if (b[nm + lrn - 1] != 0) return false;
-    for (uint32_t i = 0; i + 1 < lrn; i++) {
-        uint8_t c = b[nm + i];
-        if (c < 33 || c > 126 || c == '@') return false;
-    }
-    const long long cg = nm + lrn;
-    long long rlen = 0;
-    for (uint32_t i = 0; i < ncig; i++) {
-        uint32_t v = ld_u32(b, cg + 4LL * i), op = v & 15;
-        if (op > 8) return false;
-        if (ref_consuming(op)) rlen += v >> 4;
-    }
-    if (pos >= 0) {
-        int end = pos + (int)(rlen > 0 ? rlen : 1);
-        if (ld_u16(b, o + 14) != (uint32_t)reg2bin(pos, end)) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ bool is_record(const uint8_t* b, long long n, long long o, int n_ref) {
-    if (o < 0 || o + 36 > n) return false;
-    int bs = (int)ld_u32(b, o);
-    if (bs < 33 || bs > (1 << 22)) return false;
-    return record_rest(b, n, o, bs, n_ref);
-}
-
-// Candidate mask of 16-byte chunk c of the aligned view of data.
-__device__ __forceinline__ uint32_t chunk_records(const uint8_t* buf, long long n, long long c, int n_ref) {
-    uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
-    uintptr_t a = base + 16 * (uintptr_t)c;
-    long long start = (long long)(a - (uintptr_t)buf);
-    uint32_t w[5];
-    bool inside = start >= 0 && start + 20 <= n;
-    if (inside) {
-        uint4 v = __ldg(reinterpret_cast<const uint4*>(a));
-        w[0] = v.x;
-        w[1] = v.y;
-        w[2] = v.z;
-        w[3] = v.w;
-    }
-    // the next 4 bytes come from the neighbouring lane's first word when that lane loaded it
-    uint32_t nxt = __shfl_down_sync(FULL, w[0], 1);
-    const bool nb_inside = __shfl_down_sync(FULL, inside ? 1 : 0, 1) != 0;
-    if (!inside) {
-        for (int k = 0; k < 5; k++) {
-            uint32_t x = 0;
-            for (int t = 0; t < 4; t++) {
-                long long o = start + 4 * k + t;
-                if (o >= 0 && o < n) x |= (uint32_t)buf[o] << (8 * t);
-            }
-            w[k] = x;
-        }
-    } else {
-        w[4] = ((threadIdx.x & 31) == 31 || !nb_inside) ? ld_u32(buf, start + 16) : nxt;
-    }
-    if (start >= n || start + 16 <= 0) return 0;
-    uint32_t mask = 0;
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        uint32_t bs = __funnelshift_r(w[k >> 2], w[(k >> 2) + 1], 8 * (k & 3));
-        if (bs - 33u <= (1u << 22) - 33u) {
-            long long o = start + k;
-            if (o >= 0 && record_rest(buf, n, o, (int)bs, n_ref)) mask |= 1u << k;
-        }
-    }
-    return mask;
-}
-
-__global__ void __launch_bounds__(NT) k_rec_count(const uint8_t* buf, long long n, int n_ref, Ws w) {
-    __shared__ uint32_t red[NT / 32];
-    for (long long t = blockIdx.x; t < w.ntiles; t += gridDim.x) {
-        uint32_t c = __popc(chunk_records(buf, n, t * NT + threadIdx.x, n_ref));
-        for (int d = 16; d; d >>= 1) c += __shfl_down_sync(FULL, c, d);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t s = 0;
-            for (int i = 0; i < NT / 32; i++) s += red[i];
-            w.tile_count[t] = s;
-        }
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(FIN_NT) k_rec_tiles(Ws w, long long cap) {
-    __shared__ int64_t sm[33];
-    int64_t carry = 0;
-    for (long long b = 0; b < w.ntiles; b += FIN_NT) {
-        long long i = b + threadIdx.x;
-        int64_t v = i < w.ntiles ? (int64_t)w.tile_count[i] : 0;
-        int64_t tot;
-        int64_t x = block_exclusive_scan<FIN_NT>(v, tot, sm);
-        if (i < w.ntiles) w.tile_off[i] = carry + x;
-        carry += tot;
-    }
-    if (threadIdx.x == 0) {
-        w.meta[0] = carry;
-        w.meta[1] = carry > w.cap ? CB_ERR_TOO_MANY : (carry > cap ? CB_ERR_CAPACITY : CB_OK);
-        w.meta[2] = 0;
-    }
-}
-
-__global__ void __launch_bounds__(NT) k_rec_write(const uint8_t* buf, long long n, int n_ref, int64_t* out, Ws w) {
-    __shared__ int64_t sm[33];
-    if (w.meta[1] != CB_OK) return;
-    for (long long t = blockIdx.x; t < w.ntiles; t += gridDim.x) {
-        if (w.tile_count[t] == 0) continue;
-        long long c = t * NT + threadIdx.x;
-        uint32_t mask = chunk_records(buf, n, c, n_ref);
-        int64_t tot;
-        int64_t pos = w.tile_off[t] + block_exclusive_scan<NT>((int64_t)__popc(mask), tot, sm);
-        long long start = (long long)(((uintptr_t)buf & ~(uintptr_t)15) + 16 * (uintptr_t)c - (uintptr_t)buf);
-        while (mask) {
-            int k = __ffs(mask) - 1;
-            mask &= mask - 1;
-            out[pos++] = start + k;
-        }
-    }
-}
-
-__global__ void k_rec_links(const uint8_t* buf, const int64_t* cand, Ws w) {
-    if (w.meta[1] != CB_OK) return;
-    const long long m = w.meta[0];
-    int local = 0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < m; i += (long long)gridDim.x * blockDim.x) {
-        long long c = cand[i];
-        if (c + 4 + (long long)ld_u32(buf, c) != cand[i + 1]) local = 1;
-    }
-    if (__any_sync(FULL, local) && (threadIdx.x & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
-}
-
-__device__ __forceinline__ long long lower_bound(const int64_t* a, long long m, long long x) {
-    long long lo = 0, hi = m;
-    while (lo < hi) {
-        long long mid = (lo + hi) >> 1;
-        if (a[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(FIN_NT) k_rec_finish(const uint8_t* buf, int64_t* cand, cb_chain_summary* summary,
-                                                      Ws w) {
-    __shared__ int64_t sm[33];
-    const int tid = threadIdx.x;
-    const long long m = w.meta[0];
-    int status = (int)w.meta[1];
-    if (status == CB_OK && m > 0 && cand[0] != 0) status = CB_ERR_NO_CHAIN;
-    if (status != CB_OK || m == 0) {
-        if (tid == 0) {
-            summary->status = status;
-            summary->n_records = 0;
-            summary->tail = 0;
-            summary->n_candidates = m;
-            summary->chained = 1;
-        }
-        return;
-    }
-    if (w.meta[2] == 0) {
-        if (tid == 0) {
-            long long c = cand[m - 1];
-            summary->status = CB_OK;
-            summary->n_records = m;
-            summary->tail = c + 4 + (long long)ld_u32(buf, c);
-            summary->n_candidates = m;
-            summary->chained = 1;
-        }
-        return;
-    }
-    // pointer jumping from candidate 0 (src/cubam/_kernels.py:692-702): jump[i] is the candidate
-    // where candidate i ends, or m; mark[] the candidates reached from 0.
-    for (long long i = tid; i <= m; i += FIN_NT) {
-        long long j = m;
-        if (i < m) {
-            long long c = cand[i];
-            long long nx = c + 4 + (long long)ld_u32(buf, c);
-            if (i + 1 < m && cand[i + 1] == nx) j = i + 1;
-            else {
-                long long k = lower_bound(cand, m, nx);
-                if (k < m && cand[k] == nx) j = k;
-            }
-        }
-        w.jump[i] = j;
-        w.mark[i] = i == 0 ? 1 : 0;
-    }
-    __syncthreads();
-    int64_t* jp = w.jump;
-    int64_t* jq = w.jump2;
-    for (long long span = 1; span < m; span *= 2) {
-        for (long long i = tid; i < m; i += FIN_NT)
-            if (w.mark[i]) w.mark[jp[i]] = 1;
-        __syncthreads();
-        for (long long i = tid; i <= m; i += FIN_NT) jq[i] = jp[jp[i]];
-        __syncthreads();
-        int64_t* t = jp;
-        jp = jq;
-        jq = t;
-    }
-    // compact in place (reads of a chunk happen before its writes; writes never pass reads)
-    int64_t carry = 0, last = -1;
-    for (long long b = 0; b < m; b += FIN_NT) {
-        long long i = b + tid;
-        int64_t keep = (i < m && w.mark[i]) ? 1 : 0;
-        long long v = keep ? cand[i] : 0;
-        int64_t tot;
-        int64_t x = block_exclusive_scan<FIN_NT>(keep, tot, sm);
-        if (keep) {
-            cand[carry + x] = v;
-            if (carry + x + 1 == carry + tot) last = v;
-        }
-        carry += tot;
-        __syncthreads();
-    }
-    __shared__ long long s_last;
-    if (tid == 0) s_last = 0;  // raised with an unsigned atomicMax; candidate 0 is always on the chain
-    __syncthreads();
-    if (last >= 0) atomicMax(reinterpret_cast<unsigned long long*>(&s_last), (unsigned long long)last);
-    __syncthreads();
-    if (tid == 0) {
-        summary->status = CB_OK;
-        summary->n_records = carry;
-        summary->tail = s_last + 4 + (long long)ld_u32(buf, s_last);
-        summary->n_candidates = m;
-        summary->chained = 0;
-    }
 }
 
 // ---------------------------------------------------------------- columns
@@ -648,24 +340,6 @@ static unsigned grid_for(long long items, int threads) {
     long long cap = (long long)cb_device_sm_count() * 16;
     if (g > cap) g = cap;
     return (unsigned)(g < 1 ? 1 : g);
-}
-
-extern "C" size_t cb_record_chain_workspace_bytes(int64_t n) { return rec::ws_bytes(n < 0 ? 0 : n); }
-
-extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, int64_t* offsets, int64_t cap,
-                               cb_chain_summary* summary, void* workspace, size_t workspace_bytes, void* stream) {
-    if (n < 0 || !summary || !workspace || (n > 0 && (!data || !offsets)) || cap < 0) return CB_ERR_ARG;
-    if (workspace_bytes < rec::ws_bytes(n)) return CB_ERR_CAPACITY;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    rec::Ws w = rec::carve(workspace, data, n);
-    long long grid = w.ntiles < (long long)cb_device_sm_count() * 8 ? w.ntiles : (long long)cb_device_sm_count() * 8;
-    if (grid < 1) grid = 1;
-    rec::k_rec_count<<<(unsigned)grid, rec::NT, 0, s>>>(data, n, n_ref, w);
-    rec::k_rec_tiles<<<1, rec::FIN_NT, 0, s>>>(w, cap);
-    rec::k_rec_write<<<(unsigned)grid, rec::NT, 0, s>>>(data, n, n_ref, offsets, w);
-    rec::k_rec_links<<<grid_for(n / 37 + 1, 256), 256, 0, s>>>(data, offsets, w);
-    rec::k_rec_finish<<<1, rec::FIN_NT, 0, s>>>(data, offsets, summary, w);
-    return cb_set_error(cudaGetLastError());
 }
 
 extern "C" int cb_decode_fixed(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,

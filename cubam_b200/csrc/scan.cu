@@ -18,7 +18,6 @@ namespace cb {
 namespace scan {
 
 constexpr int NT = 256;
-constexpr int TILE = NT * 16;
 constexpr int FIN_NT = 1024;
 constexpr long long MAX_ISIZE = 1 << 16;
 

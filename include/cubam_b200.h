@@ -69,9 +69,9 @@ typedef struct cb_inflate_summary {
 typedef struct cb_chain_summary {
     int64_t n_records;    /* records on the chain from offset 0 */
     int64_t tail;         /* where the record after the last one starts (0 when there is none) */
-    int64_t n_candidates; /* offsets that pass the record predicate */
-    int32_t status;       /* CB_OK, CB_ERR_NO_CHAIN, CB_ERR_TOO_MANY or CB_ERR_CAPACITY */
-    int32_t chained;      /* 1 when every candidate was on the chain */
+    int64_t n_candidates; /* 0 when no offset passes the record predicate, else -1 (not counted) */
+    int32_t status;       /* CB_OK, CB_ERR_NO_CHAIN or CB_ERR_CAPACITY */
+    int32_t chained;      /* 1 when the parallel tile walks agreed, 0 when the chain was walked serially */
 } cb_chain_summary;
 
 /* ---- library ------------------------------------------------------------ */
@@ -135,7 +135,10 @@ int cb_inflate(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_job
 size_t cb_record_chain_workspace_bytes(int64_t n);
 
 /* Offsets of the complete records of data[0:n) on the chain from offset 0, under the reference's
- * record predicate (is_record, src/cubam/_kernels.py:250-278).  Writes offsets[0:cap) and *summary. */
+ * record predicate (is_record, src/cubam/_kernels.py:250-278): walked by 2 KB tiles in parallel and
+ * stitched, O(records).  Writes offsets[0:cap) (cap >= n / 37 + 1 always suffices) and *summary.
+ * cubam's "Too many candidates" error (more than n/32 + 1024 offsets passing the predicate) is not
+ * raised: the walk never tests every offset. */
 int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, int64_t* offsets, int64_t cap,
                     cb_chain_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
 
