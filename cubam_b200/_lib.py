@@ -70,6 +70,8 @@ _SIGNATURES = {
     "cb_scan_members_noalloc": (c_int, [P, I64, c_int, I64, P, I64, P, P]),
     "cb_inflate_workspace_bytes": (c_size_t, []),
     "cb_inflate": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, P]),
+    "cb_inflate_form": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, c_int, P]),
+    "cb_inflate_lane_slots": (I64, []),
     "cb_record_chain_workspace_bytes": (c_size_t, [I64]),
     "cb_record_chain": (c_int, [P, I64, c_int32, P, I64, P, P, c_size_t, P]),
     "cb_decode_fixed": (c_int, [P, P, I64] + [P] * 11 + [P]),

@@ -181,15 +181,21 @@ def scan_members(buf: torch.Tensor, eof: bool, out_base: int = 0, jobs_cap: int 
         return jobs, s
 
 
-def inflate_jobs(jobs: torch.Tensor, n_jobs: int, out: torch.Tensor, check_crc: bool = True) -> torch.Tensor:
-    """Launch ``cb_inflate`` of ``n_jobs`` jobs into ``out``; returns the device summary (no sync)."""
+def inflate_jobs(jobs: torch.Tensor, n_jobs: int, out: torch.Tensor, check_crc: bool = True, form: int = 0,
+                 job_status: torch.Tensor | None = None) -> torch.Tensor:
+    """Launch ``cb_inflate_form`` of ``n_jobs`` jobs into ``out``; returns the device summary (no sync).
+
+    ``form`` 0 lets the library choose (as ``cb_inflate``), 1 is one member per warp, 2 one per lane.
+    ``job_status`` (device uint32/int32 of ``n_jobs``) receives a status code per job when given.
+    """
     summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device="cuda")
     ws = _workspace(_lib.lib.cb_inflate_workspace_bytes())
-    rc = _lib.lib.cb_inflate(
-        jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc), None,
-        summ.data_ptr(), ws.data_ptr(), ws.numel(), stream_ptr(),
+    rc = _lib.lib.cb_inflate_form(
+        jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc),
+        job_status.data_ptr() if job_status is not None else None,
+        summ.data_ptr(), ws.data_ptr(), ws.numel(), int(form), stream_ptr(),
     )
-    _lib.check(rc, "cb_inflate")
+    _lib.check(rc, "cb_inflate_form")
     return summ
 
 

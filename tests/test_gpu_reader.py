@@ -170,6 +170,10 @@ def _payloads(seed: int):
     return out
 
 
+FORMS = [1, 2]  # one member per warp, one member per lane
+
+
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize(
     ("level", "strategy"),
     [
@@ -183,7 +187,7 @@ def _payloads(seed: int):
         (6, zlib.Z_FILTERED),
     ],
 )
-def test_inflate_matches_zlib(tmp_path, level, strategy):
+def test_inflate_matches_zlib(tmp_path, level, strategy, form):
     payloads, members = [], []
     for p in _payloads(level * 10 + strategy):
         try:
@@ -199,12 +203,13 @@ def test_inflate_matches_zlib(tmp_path, level, strategy):
     assert s.status == 0 and s.n_members == len(payloads)
     assert s.total_out == sum(len(p) for p in payloads)
     out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
-    summ = G.inflate_jobs(jobs, int(s.n_jobs), out, True)
+    summ = G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form)
     G.check_inflate(summ)
     assert _np(out).tobytes() == b"".join(payloads)
 
 
-def test_inflate_output_alignment_and_offsets():
+@pytest.mark.parametrize("form", FORMS)
+def test_inflate_output_alignment_and_offsets(form):
     """Members written at every output alignment (out_base offsets 0..17)."""
     payloads = _payloads(3)[:12]
     raw = b"".join(member(p) for p in payloads)
@@ -212,12 +217,13 @@ def test_inflate_output_alignment_and_offsets():
     for shift in range(18):
         jobs, s = G.scan_members(buf, True, out_base=shift)
         out = torch.zeros(shift + int(s.total_out), dtype=torch.uint8, device="cuda")
-        G.check_inflate(G.inflate_jobs(jobs, int(s.n_jobs), out, True))
+        G.check_inflate(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form))
         assert _np(out[shift:]).tobytes() == b"".join(payloads)
         assert not bool(out[:shift].any())
 
 
-def test_inflate_corrupt_members_are_errors():
+@pytest.mark.parametrize("form", FORMS)
+def test_inflate_corrupt_members_are_errors(form):
     """Damaged members fail with the inflate or CRC status, never hang or overrun."""
     rng = random.Random(7)
     data = b"".join(bytes(rng.choices(b"ACGTN\t\n", k=200)) for _ in range(50))
@@ -231,7 +237,8 @@ def test_inflate_corrupt_members_are_errors():
         buf = torch.frombuffer(bytearray(bytes(m) + G.EOF_BLOCK), dtype=torch.uint8).cuda()
         jobs, s = G.scan_members(buf, True)
         out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
-        st = int(G.read_struct(G.inflate_jobs(jobs, int(s.n_jobs), out, True), G._lib.InflateSummary).status)
+        st = int(G.read_struct(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form),
+                               G._lib.InflateSummary).status)
         d = zlib.decompressobj(-15)
         try:
             z = d.decompress(bytes(m[18:-8]), len(data) + 1)
@@ -246,6 +253,49 @@ def test_inflate_corrupt_members_are_errors():
                 assert _np(out).tobytes() == z
         seen.add(st)
     assert G._lib.INFLATE in seen
+
+
+def test_inflate_many_members_both_forms_same_codes():
+    """More members than the lane form has lanes, so lanes take member after member; some members
+    damaged.  Both forms give the payloads of the good members and the same per-job codes."""
+    rng = random.Random(11)
+    nrng = np.random.default_rng(11)
+    n = int(G._lib.lib.cb_inflate_lane_slots()) + 3000
+    assert n > 3000
+    words = [bytes(rng.choices(b"ACGT\t\n0123456789:chrXY", k=rng.randint(1, 12))) for _ in range(200)]
+    payloads, members, bad = [], [], set()
+    for i in range(n):
+        k = rng.choice([1, 2, 40, 300, 1000, 2500])
+        p = b"".join(rng.choice(words) for _ in range(k // 4 + 1))[:k]
+        if i % 97 == 5:
+            p = bytes(nrng.integers(0, 256, k, dtype=np.uint8))  # stored blocks
+        m = bytearray(member(p, rng.choice([1, 6, 9])))
+        if i % 211 == 7 and len(m) > 40:
+            m[18 + rng.randrange(len(m) - 26)] ^= 0x55
+            bad.add(i)
+        payloads.append(p)
+        members.append(bytes(m))
+    buf = torch.frombuffer(bytearray(b"".join(members) + G.EOF_BLOCK), dtype=torch.uint8).cuda()
+    jobs, s = G.scan_members(buf, True)
+    assert s.status == 0 and s.n_jobs == n
+    results = []
+    for form in FORMS:
+        out = torch.zeros(int(s.total_out), dtype=torch.uint8, device="cuda")
+        codes = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+        summ = G.read_struct(G.inflate_jobs(jobs, n, out, True, form=form, job_status=codes), G._lib.InflateSummary)
+        codes = codes.cpu().numpy()
+        assert (codes != 99).all()
+        assert int(summ.n_bad) == int((codes != 0).sum())
+        results.append((_np(out).tobytes(), codes))
+    (out1, codes1), (out2, codes2) = results
+    assert (codes1 == codes2).all()
+    assert set(np.flatnonzero(codes1)) <= bad
+    offs = np.cumsum([0] + [len(p) for p in payloads])
+    good = np.flatnonzero(codes1 == 0)
+    assert len(good) >= n - len(bad)
+    for i in good[:: max(1, len(good) // 2000)].tolist() + good[-50:].tolist():
+        assert out1[offs[i]:offs[i + 1]] == payloads[i], i
+        assert out2[offs[i]:offs[i + 1]] == payloads[i], i
 
 
 def test_records_cross_members_and_chunks(tmp_path):
