@@ -280,6 +280,10 @@ def run_ours(args):
     value = inflated * world / (ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     achieved = inflated / (inflate_ms / 1e3) / 1e9
+    from cubam_b200 import _lib
+
+    slots = int(_lib.lib.cb_inflate_lane_slots())
+    kernel = "k_inflate_lanes" if 3 * n_members >= 2 * slots else "k_inflate_warp"
 
     # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)
     plain = None
@@ -327,7 +331,7 @@ def run_ours(args):
         "stages_ms": {k: round(v, 3) for k, v in stage.items()},
         "roofline": {
             "bound": "hbm",
-            "kernel": "k_inflate",
+            "kernel": kernel,
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
