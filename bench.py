@@ -44,6 +44,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "BAM decode GB/s (uncompressed) & records/s on 1 B200"
 UNIT = "GB/s"
 FALLBACK_HBM = 6650.0
+TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9}
 
 
 def parse():
@@ -338,7 +339,9 @@ def run_ours(args):
             "frac": achieved / peak,
             "peak_kind": peak_kind,
             "algorithmic": "decompressed bytes (sum of ISIZE) per launch",
-            "traffic": None,
+            # DRAM bytes (read + write) per inflated byte of k_inflate_lanes from one ncu capture of the
+            # 4M-record GEX case (profiles/k_inflate_lanes_gex4m.md), scaled by the launch's inflated bytes
+            "traffic": inflated * TRAFFIC_PER_BYTE[kernel] if kernel in TRAFFIC_PER_BYTE else None,
         },
         "clocks": clk.summary(),
         "gpu_launches": counter.get("launches", 0),
