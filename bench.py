@@ -339,8 +339,8 @@ def run_ours(args):
             "frac": achieved / peak,
             "peak_kind": peak_kind,
             "algorithmic": "decompressed bytes (sum of ISIZE) per launch",
-            # DRAM bytes (read + write) per inflated byte of k_inflate_lanes from one ncu capture of the
-            # 4M-record GEX case (profiles/k_inflate_lanes_gex4m.md), scaled by the launch's inflated bytes
+            # DRAM bytes (read + write) per inflated byte of k_inflate_lanes, measured by ncu on the
+            # 4M-record GEX case, scaled by the launch's inflated bytes
             "traffic": inflated * TRAFFIC_PER_BYTE[kernel] if kernel in TRAFFIC_PER_BYTE else None,
         },
         "clocks": clk.summary(),
