@@ -213,3 +213,205 @@ def load_compressed(path, device="cuda") -> torch.Tensor:
     raw = np.fromfile(path, dtype=np.uint8)
     host = torch.from_numpy(raw).pin_memory()
     return host.to(device, non_blocking=True)
+
+
+class BatchPlan:
+    """A fixed set of resident files decoded by one launch sequence with no host synchronisation.
+
+    The first decode (:func:`decode_many`) sizes everything: each file's jobs, inflated bytes and
+    records.  The plan then owns every buffer (one job table and one output arena for all files,
+    per-file offsets, columns and tag columns, shared scan and chain workspaces) and
+    :meth:`launch` issues, on the current stream, the scans (each writing its jobs straight into
+    its slice of the job table, with its output base), ONE inflate launch for the members of all
+    files, the record chains, and the columns and tags.  Because nothing in it waits for the
+    host, :meth:`capture` records it as a CUDA graph and :meth:`replay` re-runs the whole batch
+    with one launch; :meth:`check` reads every device summary with one copy and raises on a
+    status or on counts that differ from the plan.
+
+    ``form`` is the inflate form (1: a member per warp, 2: a member per lane); None lets
+    :meth:`autotune` time both on this batch and keep the faster.
+    """
+
+    def __init__(self, files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "GN"), check_crc: bool = True,
+                 form: int | None = None):
+        self.files = files
+        self.tags = tuple(tags)
+        self.check_crc = check_crc
+        first = decode_many(files, tags=tags, check_crc=check_crc)
+        self.n_files = len(files)
+        self.n_members = [d.n_members for d in first]
+        self.inflated = [d.inflated_bytes for d in first]
+        self.n_records = [len(d) for d in first]
+        del first  # its buffers go back to the allocator before the plan takes its own
+        # jobs per file (members with ISIZE > 0): from a scan summary of the first pass
+        self.n_jobs = []
+        self.out_base = []
+        base = 0
+        for (comp, _), total in zip(files, self.inflated):
+            self.out_base.append(base)
+            base += total
+        self.total_out = base
+        dev = "cuda"
+        sizes = [int(c.numel()) for c, _ in files]
+        self.scan_ws = torch.empty(max([int(_lib.lib.cb_scan_workspace_bytes(n)) for n in sizes] + [256]),
+                                   dtype=torch.uint8, device=dev)
+        ssz = ctypes_sizeof(_lib.ScanSummary)
+        self.scan_summ = torch.zeros((self.n_files, ssz), dtype=torch.uint8, device=dev)
+        # count the jobs of each file with one scan pass (a cap-0 scan reports n_jobs)
+        probe = torch.empty(_lib.JOB_BYTES, dtype=torch.uint8, device=dev)
+        for k, ((comp, _), n) in enumerate(zip(files, sizes)):
+            rc = _lib.lib.cb_scan_members(comp.data_ptr() if n else None, n, 1, 0, probe.data_ptr(), 0,
+                                          self.scan_summ[k].data_ptr(), self.scan_ws.data_ptr(),
+                                          self.scan_ws.numel(), stream_ptr())
+            _lib.check(rc, "cb_scan_members")
+        infos = [_lib.ScanSummary.from_buffer_copy(r.tobytes()) for r in self.scan_summ.cpu().numpy()]
+        self.n_jobs = [int(i.n_jobs) for i in infos]
+        self.job_base = [0]
+        for nj in self.n_jobs:
+            self.job_base.append(self.job_base[-1] + nj)
+        self.jobs = torch.empty(max(self.job_base[-1], 1) * _lib.JOB_BYTES, dtype=torch.uint8, device=dev)
+        self.out = torch.empty(max(self.total_out, 1), dtype=torch.uint8, device=dev)
+        self.inflate_summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device=dev)
+        self.queue_ws = torch.empty(max(int(_lib.lib.cb_inflate_workspace_bytes()), 256), dtype=torch.uint8,
+                                    device=dev)
+        self.data = []
+        for (comp, header), b, total in zip(files, self.out_base, self.inflated):
+            self.data.append(self.out[b + header.size : b + total])
+        self.chain_ws = torch.empty(
+            max([int(_lib.lib.cb_record_chain_workspace_bytes(int(d.numel()))) for d in self.data] + [256]),
+            dtype=torch.uint8, device=dev)
+        self.chain_summ = torch.zeros((self.n_files, ctypes_sizeof(_lib.ChainSummary)), dtype=torch.uint8,
+                                      device=dev)
+        self.offsets = [torch.empty(max(n, 1), dtype=torch.int64, device=dev) for n in self.n_records]
+        self.results = []
+        k = len(self.tags)
+        self._tag_arrays = []
+        for (comp, header), data, off, nrec, nm, total in zip(files, self.data, self.offsets, self.n_records,
+                                                               self.n_members, self.inflated):
+            o = off[:nrec]
+            cols = {name: torch.empty(nrec, dtype=t, device=dev) for name, t in _TYPES.items()}
+            arrs = None
+            tag_cols = {}
+            if k:
+                arrs = (torch.empty((k, nrec), dtype=torch.uint8, device=dev),
+                        torch.empty((k, nrec), dtype=torch.int64, device=dev),
+                        torch.empty((k, nrec), dtype=torch.int32, device=dev),
+                        torch.empty((k, nrec), dtype=torch.int64, device=dev))
+                view = _View(data, o)
+                for q, t in enumerate(self.tags):
+                    tag_cols[t] = Tag._from_columns(view, t, arrs[0][q], arrs[1][q], arrs[2][q], arrs[3][q])
+            self._tag_arrays.append(arrs)
+            self.results.append(DecodedFile(header, data, o, cols, tag_cols, nm, total))
+        self.form = form
+        self.graph = None
+        if self.form is None:
+            self.autotune()
+
+    # ------------------------------------------------------------------ launches
+    def launch(self, form: int | None = None, events: StageEvents | None = None) -> None:
+        """Issue the whole batch on the current stream (no host synchronisation)."""
+        form = form or self.form or 0
+        s = stream_ptr()
+        if events:
+            events.mark("start")
+        for k, ((comp, _), n) in enumerate(zip(self.files, [int(c.numel()) for c, _ in self.files])):
+            jp = self.jobs.data_ptr() + self.job_base[k] * _lib.JOB_BYTES
+            rc = _lib.lib.cb_scan_members(comp.data_ptr() if n else None, n, 1, self.out_base[k], jp,
+                                          self.n_jobs[k], self.scan_summ[k].data_ptr(), self.scan_ws.data_ptr(),
+                                          self.scan_ws.numel(), s)
+            _lib.check(rc, "cb_scan_members")
+        if events:
+            events.mark("scanned")
+        rc = _lib.lib.cb_inflate_form(self.jobs.data_ptr(), self.job_base[-1], None, self.out.data_ptr(),
+                                      int(self.check_crc), None, self.inflate_summ.data_ptr(),
+                                      self.queue_ws.data_ptr(), self.queue_ws.numel(), int(form), s)
+        _lib.check(rc, "cb_inflate_form")
+        if events:
+            events.mark("inflated")
+        for k, ((comp, header), data, off, nrec) in enumerate(zip(self.files, self.data, self.offsets,
+                                                                   self.n_records)):
+            n = int(data.numel())
+            if n:
+                rc = _lib.lib.cb_record_chain(data.data_ptr(), n, len(header.names), off.data_ptr(), max(nrec, 1),
+                                              self.chain_summ[k].data_ptr(), self.chain_ws.data_ptr(),
+                                              self.chain_ws.numel(), s)
+                _lib.check(rc, "cb_record_chain")
+        if events:
+            events.mark("chained")
+        for k, (res, arrs, nrec) in enumerate(zip(self.results, self._tag_arrays, self.n_records)):
+            if not nrec:
+                continue
+            cols = res.columns
+            rc = _lib.lib.cb_decode_fixed(res.data.data_ptr(), res.offset.data_ptr(), nrec,
+                                          *(cols[f].data_ptr() for f in FIELDS), s)
+            _lib.check(rc, "cb_decode_fixed")
+            if arrs is not None:
+                rc = _lib.lib.cb_find_tags(res.data.data_ptr(), res.offset.data_ptr(), nrec,
+                                           "".join(self.tags).encode(), len(self.tags), *(a.data_ptr() for a in arrs),
+                                           s)
+                _lib.check(rc, "cb_find_tags")
+        if events:
+            events.mark("decoded")
+
+    def launches_per_run(self) -> int:
+        """Kernels of this library in one :meth:`launch` (the graph holds the same)."""
+        chains = sum(1 for d in self.data if int(d.numel()))
+        decodes = sum(1 for n in self.n_records if n)
+        return (KERNELS["scan"] * self.n_files + KERNELS["inflate"] + KERNELS["chain"] * chains
+                + (KERNELS["decode"] + (KERNELS["tags"] if self.tags else 0)) * decodes)
+
+    def check(self) -> None:
+        """Raise on any device status of the last run, or counts that differ from the plan (one sync)."""
+        scan = self.scan_summ.cpu().numpy()
+        chain = self.chain_summ.cpu().numpy()
+        raise_status(read_struct(self.inflate_summ, _lib.InflateSummary).status, "inflate")
+        for k in range(self.n_files):
+            si = _lib.ScanSummary.from_buffer_copy(scan[k].tobytes())
+            raise_status(si.status, "BGZF member scan")
+            if int(si.n_jobs) != self.n_jobs[k] or int(si.total_out) != self.inflated[k]:
+                raise RuntimeError(f"file {k}: the scan differs from the plan")
+            if int(self.data[k].numel()):
+                ci = _lib.ChainSummary.from_buffer_copy(chain[k].tobytes())
+                raise_status(ci.status, "record chain")
+                if int(ci.n_records) != self.n_records[k] or int(ci.tail) != int(self.data[k].numel()):
+                    raise RuntimeError(f"file {k}: the record chain differs from the plan")
+
+    # ------------------------------------------------------------------ tuning and graphs
+    def autotune(self, reps: int = 2) -> dict:
+        """Time the batch with each inflate form (members per CTA: 8 one per warp, 128 one per lane) and
+        keep the faster; returns the inflate milliseconds per form."""
+        times = {}
+        for form in (1, 2):
+            self.launch(form)
+            torch.cuda.synchronize()
+            self.check()
+            best = None
+            for _ in range(reps):
+                ev = StageEvents()
+                self.launch(form, ev)
+                torch.cuda.synchronize()
+                ms = ev.ms()["inflated"]
+                best = ms if best is None else min(best, ms)
+            times[form] = best
+        self.form = min(times, key=times.get)
+        self.tuning = times
+        return times
+
+    def capture(self) -> None:
+        """Record :meth:`launch` as a CUDA graph (after one eager run has set every kernel up)."""
+        self.launch()
+        torch.cuda.synchronize()
+        self.check()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        torch.cuda.synchronize()
+        self.graph = g
+
+    def replay(self) -> list[DecodedFile]:
+        """Re-run the whole batch (the graph when captured, else the launches); no synchronisation."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self.launch()
+        return self.results
