@@ -1,0 +1,121 @@
+"""The serving loop: each request's records, columns and tags are the same decoded alone, served in a
+mix with others (split into slices, sharing steps and inflate launches), and cut from the whole
+file's decode."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from cubam_b200 import batch, serve, synth  # noqa: E402
+from cubam_b200.synth import Config  # noqa: E402
+
+TAGS = ("CB", "UB", "GN")
+FIELDS = ("ref", "pos", "end", "mapq", "flag", "nref", "npos", "tlen", "l_seq", "clip_left", "clip_right")
+
+
+@pytest.fixture(scope="module")
+def files(tmp_path_factory):
+    d = tmp_path_factory.mktemp("serve")
+    cfgs = [Config("g", 1, 60_000, 41), Config("a", 2, 90_000, 42, n_barcodes=10_000),
+            Config("m", 1, 25_000, 43, level=-1, stored_frac=0.05)]
+    out = []
+    for c in cfgs:
+        p = d / f"{c.name}.bam"
+        synth.write_bam(p, c)
+        out.append(serve.ResidentFile.load(p))
+    return out
+
+
+def _host(res):
+    return {
+        "data": res.data.cpu().numpy().tobytes(),
+        "offset": res.offset.cpu().numpy(),
+        **{f: res.columns[f].cpu().numpy() for f in FIELDS},
+        **{f"{t}.{x}": getattr(res.tags[t], x).cpu().numpy() for t in TAGS for x in ("type", "offset", "length", "value")},
+    }
+
+
+def _equal(a, b):
+    assert a.keys() == b.keys()
+    for k in a:
+        if k == "data":
+            assert a[k] == b[k]
+        else:
+            assert np.array_equal(a[k], b[k]), k
+
+
+def _ranges(rf, rng, n):
+    ok = rf.boundaries()
+    out = [(int(ok[0]), int(ok[-1])), (int(ok[0]), int(ok[0])), (int(ok[-2]), int(ok[-1]))]
+    while len(out) < n:
+        a, b = sorted(int(x) for x in rng.choice(ok, 2, replace=False))
+        out.append((a, b))
+    return out
+
+
+def test_index_matches_the_whole_file(files):
+    for rf in files:
+        whole = batch.decode_many([(rf.comp, rf.header)], tags=())[0]
+        ix = rf.index
+        assert int(ix.cum_rec[-1]) == len(whole)
+        starts = whole.offset.cpu().numpy() + rf.header.size
+        for m in rf.boundaries()[:-1]:
+            k = int(ix.cum_rec[m])
+            assert starts[k] == ix.ucum[m] + ix.first_rec[m]
+            assert rf.member_of(rf.voff(int(m))) == m
+
+
+def test_requests_alone_match_the_whole_file(files):
+    rng = np.random.default_rng(5)
+    for rf in files:
+        whole = _host(batch.decode_many([(rf.comp, rf.header)], tags=TAGS)[0])
+        for a, b in _ranges(rf, rng, 12):
+            req = serve.Request(0, rf.voff(a), rf.voff(b))
+            got = _host(serve.decode_alone(rf, req, tags=TAGS))
+            ix = rf.index
+            r0, r1 = int(ix.cum_rec[a]), int(ix.cum_rec[b])
+            assert len(got["offset"]) == r1 - r0 == req.n_records
+            shift = int(ix.ucum[a] + ix.first_rec[a]) - rf.header.size  # request data start in the whole file
+            w0 = shift
+            assert got["data"] == whole["data"][w0 : w0 + req.inflated_bytes]
+            assert np.array_equal(got["offset"], whole["offset"][r0:r1] - shift)
+            for f in FIELDS:
+                assert np.array_equal(got[f], whole[f][r0:r1]), f
+            for t in TAGS:
+                assert np.array_equal(got[f"{t}.offset"], whole[f"{t}.offset"][r0:r1] - shift), t
+                for x in ("type", "length", "value"):
+                    assert np.array_equal(got[f"{t}.{x}"], whole[f"{t}.{x}"][r0:r1]), (t, x)
+
+
+def test_served_in_a_mix_equals_alone(files):
+    rng = np.random.default_rng(6)
+    reqs = []
+    for f, rf in enumerate(files):
+        for a, b in _ranges(rf, rng, 14):
+            reqs.append(serve.Request(f, rf.voff(a), rf.voff(b), arrival=float(rng.uniform(0, 0.05)), rid=len(reqs)))
+    alone = {r.rid: _host(serve.decode_alone(files[r.file], serve.Request(r.file, r.voff_begin, r.voff_end), TAGS))
+             for r in reqs}
+    got = {}
+
+    def on_done(r):
+        got[r.rid] = _host(r.result)
+
+    # a small budget and small slices and steps: requests wait for memory, split into several
+    # slices, and share steps with others
+    server = serve.Server(files, budget_bytes=48 << 20, step_bytes=1 << 20, slice_bytes=256 << 10, tags=TAGS)
+    done = server.run(reqs, on_done=on_done)
+    assert len(done) == len(reqs) and set(got) == {r.rid for r in reqs}
+    assert server.steps > len(reqs) // 2
+    assert max(n for n, _ in server.step_log) > 1  # steps held slices of several requests
+    assert any(len(serve.slice_request(files[r.file], r, 256 << 10)) > 2 for r in reqs)
+    assert server.alloc.free == [(0, server.pool_bytes)] and server.side_used == 0
+    for r in reqs:
+        _equal(got[r.rid], alone[r.rid])
+        assert r.done is not None and r.done >= r.arrival
+    lat = serve.latency_summary(done)
+    assert lat["all_ms"]["n"] == len(reqs)
