@@ -53,7 +53,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="gex", choices=["gex", "small", "atac", "uneven"])
+    ap.add_argument("--config", default="gex", choices=["gex", "small", "atac", "uneven", "serve"])
+    ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests")
+    ap.add_argument("--file-records", type=int, default=4_000_000, help="serve: records per resident file")
     ap.add_argument("--scale", type=float, default=1.0, help="uneven: record counts times this")
     ap.add_argument("--records", type=int, default=None, help="override the workload size (records)")
     ap.add_argument("--chunk-bytes", type=int, default=256 << 20, help="compressed chunk of the e2e read_bam")
@@ -548,9 +551,97 @@ def run_uneven(args):
     }), flush=True)
 
 
+def run_serve(args):
+    """The serving loop: 16 resident files (GEX and ATAC shapes), requests of log-uniform 64 KB-512 MB
+    compressed ranges arriving as a Poisson stream, admitted under a 40 GB HBM budget; latency
+    percentiles and throughput of continuous batching against the plain sequential decode (one
+    request at a time, in arrival order), and the saturation throughput (all requests at once)."""
+    import torch
+
+    from cubam_b200 import serve, synth
+    from cubam_b200.synth import Config
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    base = Path(args.workdir or ("/dev/shm" if Path("/dev/shm").exists() else "/tmp"))
+    t0 = time.perf_counter()
+    files = []
+    for i in range(16):
+        shape = 1 if i % 2 == 0 else 2
+        cfg = Config(f"serve{i}", shape, args.file_records, 4000 + i, n_barcodes=1000 if shape == 1 else 10_000)
+        path = base / f"cubam_bench_{cfg.name}_{cfg.n_records}_s{cfg.seed}.bam"
+        if not path.exists():
+            tmp = path.with_suffix(f".tmp{os.getpid()}")
+            synth.write_bam(tmp, cfg)
+            tmp.replace(path)
+        files.append(serve.ResidentFile.load(path))
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    tags = ("CB", "UB", "GN")
+    budget = 40 << 30
+
+    def requests(rate):
+        return serve.poisson_requests(files, args.requests, rate, seed=4)
+
+    def sink(r):  # consume the result on the device, as a caller would, then release it
+        if r.result is not None and len(r.result):
+            r.result.columns["pos"].sum()
+
+    server = serve.Server(files, budget_bytes=budget, tags=tags)
+    warm = requests(1e9)[:16]
+    server.run(warm, on_done=sink)  # set every kernel up
+    torch.cuda.synchronize()
+
+    def served(rate):
+        reqs = requests(rate)
+        with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            t = time.perf_counter()
+            done = server.run(reqs, on_done=sink, t0=t)
+            torch.cuda.synchronize()
+            span = time.perf_counter() - t
+        inflated = sum(r.inflated_bytes for r in done)
+        return {"throughput_gbs": inflated / span / 1e9, "span_s": span, "steps": server.steps,
+                **serve.latency_summary(done)}, clk.summary(), done
+
+    live, clocks, done = served(args.rate)
+    n_small = sum(1 for r in done if r.compressed_bytes <= (8 << 20))
+    sat, _, _ = served(1e9)  # every request at once: the loop's batch throughput
+
+    # the plain sequential decode: one request at a time in arrival order, each alone
+    reqs = requests(args.rate)
+    t = time.perf_counter()
+    for r in reqs:
+        now = time.perf_counter() - t
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        res = serve.decode_alone(files[r.file], r, tags=tags)
+        sink(serve.Request(0, 0, 0, result=res))
+        torch.cuda.synchronize()
+        r.done = time.perf_counter() - t
+        del res
+    span = time.perf_counter() - t
+    plain = {"throughput_gbs": sum(r.inflated_bytes for r in reqs) / span / 1e9, "span_s": span,
+             **serve.latency_summary(reqs)}
+    total = sum(r.inflated_bytes for r in done)
+    print(json.dumps({
+        "metric": METRIC, "value": live["throughput_gbs"], "unit": UNIT, "n_gpus": 1, "steps": args.requests,
+        "warmup": 16, "ms_per_step": live["span_s"] * 1e3 / args.requests, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"serve: 16 resident files x {args.file_records} records (GEX/ATAC), {args.requests} "
+                               f"requests of log-uniform 64 KB-512 MB compressed ranges, Poisson {args.rate}/s, "
+                               f"40 GB HBM budget, seed 4",
+                   "inflated_bytes_requested": total, "small_requests": n_small, "generate_s": round(gen_s, 1),
+                   "step_bytes": server.step_bytes, "slice_bytes": server.slice_bytes},
+        "served": live, "saturation": sat, "plain_sequential": plain,
+        "served_vs_saturation": live["throughput_gbs"] / sat["throughput_gbs"],
+        "clocks": clocks,
+    }), flush=True)
+
+
 def main():
     args = parse()
-    if args.config == "uneven":
+    if args.config == "serve":
+        run_serve(args)
+    elif args.config == "uneven":
         run_uneven(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -258,18 +258,19 @@ def _finish_request(req: Request, rf: ResidentFile, data: torch.Tensor, off: tor
     if n:
         rc = _lib.lib.cb_decode_fixed(data.data_ptr(), off.data_ptr(), n, *(cols[f].data_ptr() for f in FIELDS), s)
         _lib.check(rc, "cb_decode_fixed")
-        if tags:
-            k = len(tags)
-            ty = torch.empty((k, n), dtype=torch.uint8, device="cuda")
-            vo = torch.empty((k, n), dtype=torch.int64, device="cuda")
-            vl = torch.empty((k, n), dtype=torch.int32, device="cuda")
-            iv = torch.empty((k, n), dtype=torch.int64, device="cuda")
+    if tags:  # tag columns exist (empty) for a request without records too
+        k = len(tags)
+        ty = torch.empty((k, n), dtype=torch.uint8, device="cuda")
+        vo = torch.empty((k, n), dtype=torch.int64, device="cuda")
+        vl = torch.empty((k, n), dtype=torch.int32, device="cuda")
+        iv = torch.empty((k, n), dtype=torch.int64, device="cuda")
+        if n:
             rc = _lib.lib.cb_find_tags(data.data_ptr(), off.data_ptr(), n, "".join(tags).encode(), k, ty.data_ptr(),
                                        vo.data_ptr(), vl.data_ptr(), iv.data_ptr(), s)
             _lib.check(rc, "cb_find_tags")
-            view = _View(data, off)
-            for q, t in enumerate(tags):
-                tag_cols[t] = Tag._from_columns(view, t, ty[q], vo[q], vl[q], iv[q])
+        view = _View(data, off)
+        for q, t in enumerate(tags):
+            tag_cols[t] = Tag._from_columns(view, t, ty[q], vo[q], vl[q], iv[q])
     return DecodedFile(rf.header, data, off, cols, tag_cols, req.m1 - req.m0, req.inflated_bytes)
 
 
