@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="gex", choices=["gex", "small", "atac", "uneven", "serve"])
-    ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--rate", type=float, default=0.0,
+                    help="serve: Poisson arrivals per second (0: the rate that offers 80%% of the saturation throughput)")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests")
     ap.add_argument("--file-records", type=int, default=4_000_000, help="serve: records per resident file")
     ap.add_argument("--scale", type=float, default=1.0, help="uneven: record counts times this")
@@ -602,12 +603,17 @@ def run_serve(args):
         return {"throughput_gbs": inflated / span / 1e9, "span_s": span, "steps": server.steps,
                 **serve.latency_summary(done)}, clk.summary(), done
 
-    live, clocks, done = served(args.rate)
-    n_small = sum(1 for r in done if r.compressed_bytes <= (8 << 20))
     sat, _, _ = served(1e9)  # every request at once: the loop's batch throughput
+    probe = requests(1.0)
+    for r in probe:
+        serve.plan_request(files[r.file], r)
+    mean_bytes = sum(r.inflated_bytes for r in probe) / len(probe)
+    rate = args.rate or 0.8 * sat["throughput_gbs"] * 1e9 / mean_bytes
+    live, clocks, done = served(rate)
+    n_small = sum(1 for r in done if r.compressed_bytes <= (8 << 20))
 
     # the plain sequential decode: one request at a time in arrival order, each alone
-    reqs = requests(args.rate)
+    reqs = requests(rate)
     t = time.perf_counter()
     for r in reqs:
         now = time.perf_counter() - t
@@ -627,8 +633,9 @@ def run_serve(args):
         "warmup": 16, "ms_per_step": live["span_s"] * 1e3 / args.requests, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": f"serve: 16 resident files x {args.file_records} records (GEX/ATAC), {args.requests} "
-                               f"requests of log-uniform 64 KB-512 MB compressed ranges, Poisson {args.rate}/s, "
-                               f"40 GB HBM budget, seed 4",
+                               f"requests of log-uniform 64 KB-512 MB compressed ranges, Poisson {rate:.1f}/s "
+                               f"({'80% of saturation' if not args.rate else 'given'}), 40 GB HBM budget, seed 4",
+                   "offered_gbs": rate * mean_bytes / 1e9, "mean_request_inflated_bytes": mean_bytes,
                    "inflated_bytes_requested": total, "small_requests": n_small, "generate_s": round(gen_s, 1),
                    "step_bytes": server.step_bytes, "slice_bytes": server.slice_bytes},
         "served": live, "saturation": sat, "plain_sequential": plain,

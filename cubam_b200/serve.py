@@ -391,13 +391,22 @@ class Server:
                 out.append(_Slice(r, r.m0, r.m0, True))
                 r._last_launched = True
                 continue
+            # consecutive slices of the request while the step has room, as one member range
+            coff = self.files[r.file].index.coff
             ma, mb = r._slices[r._next]
-            b = int(self.files[r.file].index.coff[mb] - self.files[r.file].index.coff[ma])
+            b = int(coff[mb] - coff[ma])
             if out and total + b > self.step_bytes:
                 continue
-            last = r._next == len(r._slices) - 1
+            k = r._next + 1
+            while k < len(r._slices):
+                nb = int(coff[r._slices[k][1]] - coff[ma])
+                if total + nb > self.step_bytes:
+                    break
+                mb, b = r._slices[k][1], nb
+                k += 1
+            last = k == len(r._slices)
             out.append(_Slice(r, ma, mb, last))
-            r._next += 1
+            r._next = k
             r._last_launched = last
             total += b
         return out
