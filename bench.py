@@ -637,7 +637,8 @@ def run_serve(args):
                                f"({'80% of saturation' if not args.rate else 'given'}), 40 GB HBM budget, seed 4",
                    "offered_gbs": rate * mean_bytes / 1e9, "mean_request_inflated_bytes": mean_bytes,
                    "inflated_bytes_requested": total, "small_requests": n_small, "generate_s": round(gen_s, 1),
-                   "step_bytes": server.step_bytes, "slice_bytes": server.slice_bytes},
+                   "step_bytes": server.long_step_bytes, "short_step_bytes": server.short_step_bytes,
+                   "slice_bytes": server.slice_bytes},
         "served": live, "saturation": sat, "plain_sequential": plain,
         "served_vs_saturation": live["throughput_gbs"] / sat["throughput_gbs"],
         "clocks": clocks,

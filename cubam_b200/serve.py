@@ -324,15 +324,21 @@ class Server:
     """Continuous batching of decode requests (see the module docstring).
 
     ``budget_bytes`` is the HBM the in-flight requests may hold: the pool for their inflated bytes
-    is ``pool_frac`` of it, the rest bounds their offsets, columns and tags.
+    is ``pool_frac`` of it, the rest bounds their offsets, columns and tags.  A step holds up to
+    ``step_bytes`` compressed bytes, or ``short_step_bytes`` while a request of at most
+    ``small_bytes`` waits to start: shorter steps for a small request's latency, longer ones for
+    throughput.
     """
 
-    def __init__(self, files: list[ResidentFile], budget_bytes: int = 40 << 30, step_bytes: int = 192 << 20,
+    def __init__(self, files: list[ResidentFile], budget_bytes: int = 40 << 30, step_bytes: int = 320 << 20,
                  slice_bytes: int = 48 << 20, tags=("CB", "UB", "GN"), check_crc: bool = True,
-                 pool_frac: float = 0.7):
+                 pool_frac: float = 0.7, short_step_bytes: int = 128 << 20, small_bytes: int = 8 << 20):
         self.files = files
         self.tags = tuple(tags)
         self.check_crc = check_crc
+        self.long_step_bytes = int(step_bytes)
+        self.short_step_bytes = min(int(short_step_bytes), int(step_bytes))
+        self.small_bytes = int(small_bytes)
         self.step_bytes = int(step_bytes)
         self.slice_bytes = int(slice_bytes)
         self.pool_bytes = int(budget_bytes * pool_frac) & ~255
@@ -384,6 +390,9 @@ class Server:
         ready = [r for r in self.active if not r._last_launched]
         if not ready:
             return []
+        small_waiting = any(r.compressed_bytes <= self.small_bytes and r._next == 0 for r in ready) or any(
+            r.compressed_bytes <= self.small_bytes for r in self.pending)
+        self.step_bytes = self.short_step_bytes if small_waiting else self.long_step_bytes
         order = [ready[0]] + sorted(ready[1:], key=remaining)
         out, total = [], 0
         for r in order:
