@@ -254,15 +254,33 @@ def _inflate(path: str | Path, chunk_bytes: int | None, prefix, check_crc: bool 
     chunk_bytes = chunk_bytes or auto_chunk_bytes()
     reader = _ChunkReader(path, chunk_bytes, **reader_kw)
     carry = torch.empty(0, dtype=torch.uint8, device="cuda")
+    copies = torch.cuda.Stream()  # host-to-device copies of the next chunk overlap the work on this one
+
+    def upload(item):
+        slot, nbytes, eof = item
+        dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        copies.wait_stream(torch.cuda.current_stream())  # dev's memory may have been in use there
+        with torch.cuda.stream(copies):
+            dev.copy_(reader.host(slot)[:nbytes], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(copies)
+        return slot, eof, dev, ev
+
     try:
-        for slot, nbytes, eof in reader:
-            buf = torch.empty(int(carry.numel()) + nbytes, dtype=torch.uint8, device="cuda")
+        chunks = iter(reader)
+        first = next(chunks, None)
+        cur = upload(first) if first is not None else None
+        while cur is not None:
+            slot, eof, dev, ev = cur
+            ev.synchronize()
+            reader.release(slot)  # the host slot is copied: the reader may fill it again
+            nxt = next(chunks, None)
+            cur = upload(nxt) if nxt is not None else None
+            torch.cuda.current_stream().wait_event(ev)
             c = int(carry.numel())
-            if c:
-                buf[:c].copy_(carry)
-            buf[c:].copy_(reader.host(slot)[:nbytes], non_blocking=True)
-            res = _inflate_blocks(buf, eof, prefix and prefix(), check_crc, defer_check)  # syncs: the copy is done
-            reader.release(slot)
+            buf = torch.cat([carry, dev]) if c else dev
+            del dev
+            res = _inflate_blocks(buf, eof, prefix and prefix(), check_crc, defer_check)
             data, used = res[0], res[1]
             carry = buf[used:].clone()
             del buf
