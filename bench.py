@@ -70,6 +70,24 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(ms: float) -> float:
+    """The largest of the ranks' times (every rank gets it): NCCL on the GPU, gloo on the host."""
+    import torch
+    import torch.distributed as td
+
+    if not (td.is_available() and td.is_initialized()) or td.get_world_size() == 1:
+        return ms
+    dev = "cuda" if td.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job(units_per_rank: float, ms: float, world: int) -> float:
+    """Weak scaling: every rank processed the same units; the job's rate over the slowest rank's time."""
+    return units_per_rank * world / (ms / 1e3)
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -276,14 +294,10 @@ def run_ours(args):
         barrier()
     ms = start.elapsed_time(stop) / args.steps
     if dist:
-        import torch.distributed as td
-
-        t = torch.tensor([ms], device="cuda")
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
     stage = {k: statistics.mean(e.ms()[k] for e in evs) for k in evs[0].ms()}
     inflate_ms = stage["inflated"]
-    value = inflated * world / (ms / 1e3) / 1e9
+    value = whole_job(inflated, ms, world) / 1e9
     peak, peak_kind = peaks()
     achieved = inflated / (inflate_ms / 1e3) / 1e9
     from cubam_b200 import _lib
@@ -449,11 +463,7 @@ def run_e2e(path, args, tags, inflated, rank, dist):
     ms = s.elapsed_time(e) / args.e2e_steps
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if dist:
-        import torch.distributed as td
-
-        t = torch.tensor([ms], device="cuda")
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
     return {
         "value": inflated * world / (ms / 1e3) / 1e9,
         "unit": UNIT,
