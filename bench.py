@@ -300,10 +300,7 @@ def run_ours(args):
     value = whole_job(inflated, ms, world) / 1e9
     peak, peak_kind = peaks()
     achieved = inflated / (inflate_ms / 1e3) / 1e9
-    from cubam_b200 import _lib
-
-    slots = int(_lib.lib.cb_inflate_lane_slots())
-    kernel = "k_inflate_lanes" if 3 * n_members >= 2 * slots else "k_inflate_warp"
+    kernel = "k_inflate_warp"  # the form cb_inflate runs
 
     # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)
     plain = None

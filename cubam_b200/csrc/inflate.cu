@@ -7,13 +7,13 @@
 // Huffman decoding is serial within a member; the parallelism is across members.  Two forms, both
 // persistent grids that take members from a work queue, with the same per-member results:
 //
-//  1. one member per warp (k_inflate_warp): the warp reads the bit stream in lock step, decodes a
-//     batch of symbols into tokens and writes them warp-parallel; a member finishes soonest this
-//     way, so it serves batches with fewer members than the GPU has decoder lanes.
+//  1. one member per warp (k_inflate_warp, 32 warps per SM): the warp reads the bit stream in lock
+//     step, decodes a batch of symbols into tokens and writes them warp-parallel.
 //  2. one member per lane (k_inflate_lanes): 8 lanes of each of 16 warps per SM each inflate a
-//     member of their own, 128 members per SM in flight; it serves large batches.
+//     member of their own, 128 members per SM in flight.
 //
-// cb_inflate picks the form from the member count; cb_inflate_form takes it from the caller.
+// cb_inflate runs form 1 (the faster at every batch size measured); cb_inflate_form takes the form
+// from the caller.
 //
 // Every loop is bounded by the member's sizes or a fixed count: output beyond ISIZE, a distance
 // before the member's start, bits read beyond the payload, bad code lengths and invalid symbols are
@@ -24,8 +24,8 @@
 namespace cb {
 namespace infl {
 
-constexpr int LB = 10;                    // literal/length root bits (form 1)
-constexpr int DB = 8;                     // distance root bits (form 1)
+constexpr int LB = 8;                     // literal/length root bits (form 1)
+constexpr int DB = 7;                     // distance root bits (form 1)
 constexpr int CLB = 7;                    // code-length code bits
 constexpr int WIN = 1024;                 // form 1 flush / CRC window
 constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << DB) - 1;
@@ -436,8 +436,8 @@ template <class WS> __device__ uint32_t read_tables(Reader& r, WS& W, uint32_t b
 namespace wm {
 
 constexpr int WARPS = 8;
-constexpr int NTOK = 512;                 // tokens decoded before a batch is written
-constexpr uint32_t RING = 4096;
+constexpr int NTOK = 128;                 // tokens decoded before a batch is written
+constexpr uint32_t RING = 2048;
 constexpr uint32_t GROUP = 512;           // a group of tokens starts within this many output bytes
 static_assert(RING >= GROUP + 258 + WIN + 16, "ring must hold a group and an unflushed window");
 
@@ -1181,7 +1181,7 @@ __device__ void init_crc8(uint32_t (*crc8)[256]) {
     }
 }
 
-__global__ void __launch_bounds__(wm::WARPS * 32, 2)
+__global__ void __launch_bounds__(wm::WARPS * 32, 4)
     k_inflate_warp(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
                    uint8_t* out_base, int check_crc, uint32_t* job_status, cb_inflate_summary* summary,
                    unsigned long long* queue) {
@@ -1440,10 +1440,7 @@ extern "C" int cb_inflate_form(const cb_member_job* jobs, int64_t n_jobs, const 
                                int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
                                size_t workspace_bytes, int form, void* stream) {
     if (!summary || !workspace || workspace_bytes < cb_inflate_workspace_bytes() || n_jobs < 0) return CB_ERR_ARG;
-    if (form == 0) {
-        const int64_t slots = cb_inflate_lane_slots();
-        form = (slots > 0 && 3 * n_jobs >= 2 * slots) ? 2 : 1;
-    }
+    if (form == 0) form = 1;  // measured ahead of form 2 from 7.7 k to 193 k members (GEX, B200)
     if (form != 1 && form != 2) return CB_ERR_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     auto* queue = reinterpret_cast<unsigned long long*>(workspace);

@@ -124,16 +124,15 @@ size_t cb_inflate_workspace_bytes(void);
  * out_base + jobs[i].out_off with a persistent grid that takes members from a work queue.
  * When d_n_jobs is not NULL the job count is read from device memory (n_jobs is then the
  * capacity).  Each member must give exactly isize bytes; with check_crc its CRC32 must match.
- * job_status (device, may be NULL) gets a code per job.  The form is chosen from n_jobs: one
- * member per lane when n_jobs is at least 2/3 of cb_inflate_lane_slots(), else one per warp. */
+ * job_status (device, may be NULL) gets a code per job.  Runs the one-member-per-warp form
+ * (cb_inflate_form with form 1). */
 int cb_inflate(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
                uint32_t* job_status, cb_inflate_summary* summary, void* workspace, size_t workspace_bytes,
                void* stream);
 
-/* cb_inflate with the form given: 1 = one member per warp (a member finishes soonest),
- * 2 = one member per lane (most members in flight), 0 = chosen as cb_inflate does.  Both forms
- * give the same bytes and the same per-job codes.  No cubam counterpart (cubam has one
- * nvCOMP call, src/cubam/bgzf.py:595). */
+/* cb_inflate with the form given: 1 = one member per warp, 2 = one member per lane (most
+ * members in flight), 0 = as cb_inflate.  Both forms give the same bytes and the same per-job
+ * codes.  No cubam counterpart (cubam has one nvCOMP call, src/cubam/bgzf.py:595). */
 int cb_inflate_form(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
                     int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
                     size_t workspace_bytes, int form, void* stream);
