@@ -44,7 +44,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "BAM decode GB/s (uncompressed) & records/s on 1 B200"
 UNIT = "GB/s"
 FALLBACK_HBM = 6650.0
-TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9}
+TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9,
+                    "k_inflate_warp": (1.556828e9 + 1.001137e9) / 1.008824685e9}
 
 
 def parse():
@@ -355,7 +356,7 @@ def run_ours(args):
             "frac": achieved / peak,
             "peak_kind": peak_kind,
             "algorithmic": "decompressed bytes (sum of ISIZE) per launch",
-            # DRAM bytes (read + write) per inflated byte of k_inflate_lanes, measured by ncu on the
+            # DRAM bytes (read + write) per inflated byte of the kernel, measured by ncu on the
             # 4M-record GEX case, scaled by the launch's inflated bytes
             "traffic": inflated * TRAFFIC_PER_BYTE[kernel] if kernel in TRAFFIC_PER_BYTE else None,
         },
