@@ -602,13 +602,16 @@ def run_serve(args):
 
     def served(rate):
         reqs = requests(rate)
+        steps0, gpu0, host0 = server.steps, server.gpu_ms, dict(server.host_s)
         with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
             t = time.perf_counter()
             done = server.run(reqs, on_done=sink, t0=t)
             torch.cuda.synchronize()
             span = time.perf_counter() - t
         inflated = sum(r.inflated_bytes for r in done)
-        return {"throughput_gbs": inflated / span / 1e9, "span_s": span, "steps": server.steps,
+        return {"throughput_gbs": inflated / span / 1e9, "span_s": span, "steps": server.steps - steps0,
+                "gpu_step_ms": server.gpu_ms - gpu0,
+                "host_s": {k: round(v - host0[k], 4) for k, v in server.host_s.items()},
                 **serve.latency_summary(done)}, clk.summary(), done
 
     sat, _, _ = served(1e9)  # every request at once: the loop's batch throughput

@@ -352,6 +352,8 @@ class Server:
         self.scratch = (_Scratch(), _Scratch())
         self.steps = 0
         self.step_log = []
+        self.host_s = {"plan": 0.0, "launch": 0.0, "wait": 0.0, "complete": 0.0}  # host seconds per loop phase
+        self.gpu_ms = 0.0  # device time of the steps (first to last kernel of each)
 
     # -------------------------------------------------------------- admission and planning
     def submit(self, req: Request) -> None:
@@ -422,6 +424,8 @@ class Server:
 
     # -------------------------------------------------------------- one step
     def _launch(self, slices: list[_Slice]):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
         s = stream_ptr()
         scratch = self.scratch[self.steps % 2]  # the step before may still be read back by the host
         rows = []
@@ -469,9 +473,9 @@ class Server:
                 data = self.pool[r_start : r_start + r.inflated_bytes]
                 r.result = _finish_request(r, rf, data, r._off[: r.n_records], self.tags, s)
                 done.append(r)
-        ev = torch.cuda.Event()
+        ev = torch.cuda.Event(enable_timing=True)
         ev.record()
-        return ev, n_jobs, checks, done, summ, csumm
+        return ev, n_jobs, checks, done, summ, csumm, ev0
 
     def _check(self, n_jobs, checks, summ, csumm) -> None:
         if n_jobs:
@@ -526,21 +530,32 @@ class Server:
                 if keep is not False:
                     self.release(r)
 
+        clock = time.perf_counter
         while i < len(incoming) or self.pending or self.active or inflight:
+            ta = clock()
             arrivals()
             self._admit()
             launched = False
             if len(inflight) < 2:
                 nxt = self._pick()
+                tb = clock()
+                self.host_s["plan"] += tb - ta
                 if nxt:
                     inflight.append(self._launch(nxt))
                     self.steps += 1
                     self.step_log.append((len(nxt), inflight[-1][1]))
                     launched = True
+                self.host_s["launch"] += clock() - tb
             if inflight and (len(inflight) == 2 or not launched):
                 if len(inflight) == 2 or inflight[0][0].query():
+                    tc = clock()
                     inflight[0][0].synchronize()
-                    complete(inflight.pop(0))
+                    td = clock()
+                    self.host_s["wait"] += td - tc
+                    step = inflight.pop(0)
+                    self.gpu_ms += step[6].elapsed_time(step[0])
+                    complete(step[:6])
+                    self.host_s["complete"] += clock() - td
                 else:
                     time.sleep(0.0002)
             elif not inflight and not launched and i < len(incoming):
