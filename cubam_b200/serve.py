@@ -249,6 +249,14 @@ class _Scratch:
             self.bufs[name] = b
         return b
 
+    def host(self, name: str, nbytes: int) -> torch.Tensor:
+        """A pinned host buffer (the step that last used it has completed before it is reused)."""
+        b = self.bufs.get(name)
+        if b is None or b.numel() < nbytes:
+            b = torch.empty(max(int(nbytes * 1.25), 256), dtype=torch.uint8, pin_memory=True)
+            self.bufs[name] = b
+        return b
+
 
 def _finish_request(req: Request, rf: ResidentFile, data: torch.Tensor, off: torch.Tensor, tags, s) -> DecodedFile:
     """Columns and tags of a request whose records are all chained (launches only)."""
@@ -473,16 +481,24 @@ class Server:
                 data = self.pool[r_start : r_start + r.inflated_bytes]
                 r.result = _finish_request(r, rf, data, r._off[: r.n_records], self.tags, s)
                 done.append(r)
+        # the step's summaries go to pinned host memory behind its kernels: reading them needs only the
+        # step's event, not a copy that would also wait for the step queued after it
+        isz = ctypes_sizeof(_lib.InflateSummary)
+        ncs = csz * max(len(slices), 1)
+        host = scratch.host("summaries", isz + ncs)
+        host[:isz].copy_(summ[:isz], non_blocking=True)
+        host[isz : isz + ncs].copy_(csumm[:ncs], non_blocking=True)
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
-        return ev, n_jobs, checks, done, summ, csumm, ev0
+        return ev, n_jobs, checks, done, host[:isz], host[isz : isz + ncs], ev0
 
     def _check(self, n_jobs, checks, summ, csumm) -> None:
+        """Statuses of a completed step from its summaries in pinned host memory."""
         if n_jobs:
-            raise_status(read_struct(summ, _lib.InflateSummary).status, "inflate")
+            raise_status(_lib.InflateSummary.from_buffer_copy(summ.numpy().tobytes()).status, "inflate")
         if checks:
             csz = ctypes_sizeof(_lib.ChainSummary)
-            raw = csumm[: csz * (max(k for k, _, _ in checks) + 1)].cpu().numpy()
+            raw = csumm[: csz * (max(k for k, _, _ in checks) + 1)].numpy()
             for k, nrec, n in checks:
                 cs = _lib.ChainSummary.from_buffer_copy(raw[k * csz : (k + 1) * csz].tobytes())
                 raise_status(cs.status, "record chain")
