@@ -30,6 +30,7 @@ constexpr int CLB = 7;                    // code-length code bits
 constexpr int WIN = 1024;                 // form 1 flush / CRC window
 constexpr uint32_t LMASK = (1u << LB) - 1, DMASK = (1u << DB) - 1;
 static_assert(WIN == 32 * 32, "one 32-byte CRC column per lane");
+static_assert(15 - LB <= 8 && 15 - DB <= 8 && LB >= DB, "limits of the longer codes fit their arrays");
 
 enum : uint32_t { K_LIT = 0, K_LEN = 1, K_EOB = 2, K_SLOW = 3, K_BAD = 4 };
 
@@ -169,10 +170,13 @@ __device__ __forceinline__ uint32_t sym_entry(int kind, uint32_t s, uint32_t L) 
     return entry(L, K_BAD, 0, 0);
 }
 
-// Canonical Huffman table of lens[0:nsym): tab[2^lb] indexed by the next lb bits, count[16] and
-// sorted[] for the slow path.  Returns false for an over-subscribed code, or an incomplete one
-// except a single code of length 1 (literal/length and distance codes), as zlib's inflate accepts.
-__device__ __noinline__ bool build_table(const uint8_t* lens, int nsym, int lb, int kind, uint32_t* tab, uint16_t* count,
+// Canonical Huffman table of lens[0:nsym): tab[2^lb] indexed by the next lb bits; for the codes
+// longer than lb bits, sorted[] (the symbols in canonical order) and, for code length lb + 1 + i,
+// lim[i] = (end of the length's codes, left-justified to 15 bits) | (index of its first code in
+// sorted[] minus its first code) << 16.  Returns false for an over-subscribed code, or an
+// incomplete one except a single code of length 1 (literal/length and distance codes), as zlib's
+// inflate accepts.
+__device__ __noinline__ bool build_table(const uint8_t* lens, int nsym, int lb, int kind, uint32_t* tab, uint32_t* lim,
                             uint16_t* sorted, uint32_t* scratch) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) scratch[lane] = 0;
@@ -208,7 +212,11 @@ __device__ __noinline__ bool build_table(const uint8_t* lens, int nsym, int lb, 
         scratch[16 + lane] = my_first;  // first code of the length
         scratch[32 + lane] = my_index;  // first index of the length
     }
-    if (lane < 16 && count) count[lane] = (uint16_t)cnt;
+    if (lim && lane > lb && lane < 16) {
+        const uint32_t limit = (my_first + cnt) << (15 - lane);
+        const int base = (int)my_index - (int)my_first;
+        lim[lane - lb - 1] = (limit & 0xFFFFu) | ((uint32_t)(uint16_t)(int16_t)base << 16);
+    }
     if (incomplete || maxlen == 0) {
         const uint32_t bad = entry(1, K_BAD, 0, 0);
         for (int i = lane; i < (1 << lb); i += 32) tab[i] = bad;
@@ -241,20 +249,23 @@ __device__ __noinline__ bool build_table(const uint8_t* lens, int nsym, int lb, 
     return true;
 }
 
-// Canonical decode of a code longer than the root bits (the same in every lane).  Returns the
-// table entry of the symbol, with its full code length.
-__device__ __forceinline__ uint32_t slow_decode(uint64_t bb, const uint16_t* count, const uint16_t* sorted, int kind) {
-    int code = 0, first = 0, index = 0;
-    for (int L = 1; L < 16; L++) {
-        code |= (int)((bb >> (L - 1)) & 1u);
-        int c = count[L];
-        if (code - c < first) return sym_entry(kind, sorted[index + (code - first)], (uint32_t)L);
-        index += c;
-        first += c;
-        first <<= 1;
-        code <<= 1;
+// The table entry, with its full code length, of a code longer than the root bits (N = 15 - root
+// bits): x holds at least the next 15 bits.  The same in every lane.
+template <int N>
+__device__ __forceinline__ uint32_t slow_decode(uint32_t x, const uint32_t* lim, const uint16_t* sorted, int nsym,
+                                                int kind) {
+    const uint32_t c = __brev(x) >> 17;  // the next 15 bits, first bit highest
+    int idx = -1;
+    uint32_t L = 0;
+#pragma unroll
+    for (int i = N - 1; i >= 0; i--) {
+        const uint32_t e = lim[i];
+        if (c < (e & 0xFFFFu)) {
+            idx = (int)(int16_t)(e >> 16) + (int)(c >> (N - 1 - i));
+            L = (uint32_t)(16 - N + i);
+        }
     }
-    return entry(1, K_BAD, 0, 0);
+    return (idx >= 0 && idx < nsym) ? sym_entry(kind, sorted[idx], L) : entry(1, K_BAD, 0, 0);
 }
 
 __device__ __forceinline__ bool tok_match(uint32_t t) { return (t & 0x80000000u) != 0; }
@@ -363,8 +374,8 @@ template <class WS> __device__ uint32_t read_tables(Reader& r, WS& W, uint32_t b
         for (int s = lane; s < 288; s += 32) W.lens[s] = s < 144 ? 8 : s < 256 ? 9 : s < 280 ? 7 : 8;
         for (int s = lane; s < 32; s += 32) W.lens[288 + s] = 5;
         __syncwarp();
-        if (!build_table(W.lens, 288, LB, T_LIT, W.lit, W.lcount, W.lsorted, W.scratch)) return CB_ERR_INFLATE;
-        if (!build_table(W.lens + 288, 32, DB, T_DIST, W.dist, W.dcount, W.dsorted, W.scratch))
+        if (!build_table(W.lens, 288, LB, T_LIT, W.lit, W.llim, W.lsorted, W.scratch)) return CB_ERR_INFLATE;
+        if (!build_table(W.lens + 288, 32, DB, T_DIST, W.dist, W.dlim, W.dsorted, W.scratch))
             return CB_ERR_INFLATE;
     } else {
         // dynamic block header
@@ -419,8 +430,8 @@ template <class WS> __device__ uint32_t read_tables(Reader& r, WS& W, uint32_t b
         }
         __syncwarp();
         if (L[256] == 0) return CB_ERR_INFLATE;  // no end-of-block code
-        if (!build_table(L, (int)hlit, LB, T_LIT, W.lit, W.lcount, W.lsorted, W.scratch)) return CB_ERR_INFLATE;
-        if (!build_table(L + hlit, (int)hdist, DB, T_DIST, W.dist, W.dcount, W.dsorted, W.scratch))
+        if (!build_table(L, (int)hlit, LB, T_LIT, W.lit, W.llim, W.lsorted, W.scratch)) return CB_ERR_INFLATE;
+        if (!build_table(L + hlit, (int)hdist, DB, T_DIST, W.dist, W.dlim, W.dsorted, W.scratch))
             return CB_ERR_INFLATE;
     }
     return CB_OK;
@@ -447,8 +458,8 @@ struct WarpSmem {
     uint32_t scratch[48];
     uint16_t lsorted[288];
     uint16_t dsorted[32];
-    uint16_t lcount[16];
-    uint16_t dcount[16];
+    uint32_t llim[8];            // limits of the literal/length codes longer than LB bits
+    uint32_t dlim[8];            // limits of the distance codes longer than DB bits
     uint8_t lens[352];
     uint32_t tok[NTOK];
     alignas(16) uint8_t ring[RING];
@@ -480,26 +491,48 @@ __device__ uint32_t materialize(int nt, Out& o, wm::WarpSmem& W, const wm::CtaSm
         const bool is_m = valid && tok_match(tk);
         const uint32_t dist = is_m ? tok_dist(tk) : 0u;
         if (__any_sync(FULL, valid && (q + len > o.isize || dist > q))) return CB_ERR_INFLATE;
-        if (valid && !is_m) W.ring[slot_of<wm::RING>(q + o.a)] = (uint8_t)tk;
-        __syncwarp();
         const uint32_t q1 = o.p + glen;
         const long long lim = (long long)q1 - (long long)wm::RING;  // sources below it: flushed, in HBM
-        bool pend = is_m;
-        for (int it = 0; it < 33; it++) {
-            if (!__any_sync(FULL, pend)) break;
-            const uint32_t P = __reduce_min_sync(FULL, pend ? q : 0xFFFFFFFFu);
-            const bool ready = pend && (q - dist + min(len, dist) <= P);
-            if (ready) {
-                const uint32_t src = q - dist;
-                // an overlapping copy (dist < len) reads bytes this loop wrote before
-                for (uint32_t j = 0; j < len; j++) {
-                    const uint32_t x = src + j;
-                    const uint8_t v = (long long)x >= lim ? W.ring[slot_of<wm::RING>(x + o.a)] : o.out[x];
-                    W.ring[slot_of<wm::RING>(q + j + o.a)] = v;
+        // the group's bytes, 32 at a time: lane j writes byte r0 + j.  Its symbol is found by a binary
+        // search over the symbols' offsets; a literal gives the byte, a match byte is the byte dist
+        // before it -- in the ring or HBM when that lies before this round, else the byte another lane
+        // computes in this round (pointer jumping: at most 5 exchanges for a chain of 31)
+        for (uint32_t r0 = 0; r0 < glen; r0 += 32) {
+            const uint32_t rel = r0 + lane;
+            const bool act = rel < glen;
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const int c = k + step;
+                const uint32_t exc = __shfl_sync(FULL, ex, c & 31);
+                if (c < gcount && exc <= rel) k = c;
+            }
+            const uint32_t tkk = __shfl_sync(FULL, tk, k);
+            const uint32_t b = o.p + rel;
+            const uint32_t base = o.p + r0;
+            uint32_t val = tkk & 0xFFu;
+            int src = lane;  // lane of this round that holds the byte's source (itself: resolved)
+            if (act && tok_match(tkk)) {
+                const uint32_t x = b - tok_dist(tkk);
+                if (x >= base) src = (int)(x - base);
+                else val = (long long)x >= lim ? W.ring[slot_of<wm::RING>(x + o.a)] : o.out[x];
+            }
+            bool need = src != lane;
+            for (int it = 0; it < 6 && __any_sync(FULL, need); it++) {
+                const uint32_t v2 = __shfl_sync(FULL, val, src);
+                const int s2 = __shfl_sync(FULL, src, src);
+                const bool n2 = __shfl_sync(FULL, (int)need, src) != 0;
+                if (need) {
+                    if (!n2) {
+                        val = v2;
+                        need = false;
+                    } else {
+                        src = s2;
+                    }
                 }
             }
+            if (act) W.ring[slot_of<wm::RING>(b + o.a)] = (uint8_t)val;
             __syncwarp();
-            pend = pend && !ready;
         }
         o.p = q1;
         flush_ready<wm::RING>(o, W, S, crc);
@@ -553,7 +586,7 @@ __device__ uint32_t lock_block(Reader& r, long long in_bits, Out& o, wm::WarpSme
                 continue;
             }
             if (kind == K_SLOW) {
-                e = slow_decode((uint64_t)x, W.lcount, W.lsorted, T_LIT);
+                e = slow_decode<15 - LB>(x, W.llim, W.lsorted, 288, T_LIT);
                 kind = e_kind(e);
                 if (kind == K_LIT) {
                     advance(e_bits(e));
@@ -573,7 +606,7 @@ __device__ uint32_t lock_block(Reader& r, long long in_bits, Out& o, wm::WarpSme
             advance(cb + ext);
             const uint32_t y = __funnelshift_r(lo, hi, off);
             uint32_t d = W.dist[y & DMASK];
-            if (e_kind(d) == K_SLOW) d = slow_decode((uint64_t)y, W.dcount, W.dsorted, T_DIST);
+            if (e_kind(d) == K_SLOW) d = slow_decode<15 - DB>(y, W.dlim, W.dsorted, 32, T_DIST);
             if (e_kind(d) != K_LEN) return CB_ERR_INFLATE;
             const uint32_t db = e_bits(d), dext = e_extra(d);
             const uint32_t dist = e_value(d) + ((y >> db) & ((1u << dext) - 1u));
