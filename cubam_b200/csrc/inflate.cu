@@ -576,15 +576,17 @@ __device__ uint32_t lock_block(Reader& r, long long in_bits, Out& o, wm::WarpSme
         int nt = 0;
         bool eob = false;
         while (nt < wm::NTOK) {
-            const uint32_t x = __funnelshift_r(lo, hi, off);
+            uint32_t x = __funnelshift_r(lo, hi, off);
             uint32_t e = W.lit[x & LMASK];
-            uint32_t kind = e_kind(e);
-            if (kind == K_LIT) {
+            while (e_kind(e) == K_LIT) {  // a run of literals: the tight loop of the common case
                 advance(e_bits(e));
                 if (lane == 0) W.tok[nt] = e_value(e);
-                nt++;
-                continue;
+                if (++nt == wm::NTOK) break;
+                x = __funnelshift_r(lo, hi, off);
+                e = W.lit[x & LMASK];
             }
+            if (nt == wm::NTOK) break;
+            uint32_t kind = e_kind(e);
             if (kind == K_SLOW) {
                 e = slow_decode<15 - LB>(x, W.llim, W.lsorted, 288, T_LIT);
                 kind = e_kind(e);
