@@ -45,7 +45,7 @@ METRIC = "BAM decode GB/s (uncompressed) & records/s on 1 B200"
 UNIT = "GB/s"
 FALLBACK_HBM = 6650.0
 TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9,
-                    "k_inflate_warp": (1.556828e9 + 1.001137e9) / 1.008824685e9}
+                    "k_inflate_warp": (1.593613e9 + 1.004537e9) / 1.008824685e9}
 
 
 def parse():
