@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from cubam_b200.bam import FIELDS, Tag
+from cubam_b200.bam import FIELDS, Tag, _index
 from cubam_b200.batch import DecodedFile, _View, decode_many
 from cubam_b200.serve import Request, ResidentFile, decode_alone
 
@@ -274,8 +274,9 @@ def fetch(rf: ResidentFile, index: BaiIndex, ref: int | str, beg: int, end: int,
     keep = (c["ref"].to(torch.int64) == ref) & (pos < end) & (e > beg)
     sel = torch.nonzero(keep).flatten()
     off = res.offset[sel]
-    cols = {k: c[k][sel] for k in FIELDS}
+    cols = {k: _index(c[k], sel) for k in FIELDS}
     view = _View(res.data, off)
-    tag_cols = {t: Tag._from_columns(view, t, T.type[sel], T.offset[sel], T.length[sel], T.value[sel])
+    tag_cols = {t: Tag._from_columns(view, t, _index(T.type, sel), _index(T.offset, sel), _index(T.length, sel),
+                                     _index(T.value, sel))
                 for t, T in res.tags.items()}
     return DecodedFile(rf.header, res.data, off, cols, tag_cols, res.n_members, res.inflated_bytes)
