@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="gex", choices=["gex", "small", "atac", "uneven", "serve"])
+    ap.add_argument("--config", default="gex", choices=["gex", "small", "atac", "uneven", "serve", "bai"])
     ap.add_argument("--rate", type=float, default=0.0,
                     help="serve: Poisson arrivals per second (0: the rate that offers 80%% of the saturation throughput)")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests")
@@ -656,9 +656,64 @@ def run_serve(args):
     }), flush=True)
 
 
+def run_bai(args):
+    """Region access through a BAI index on the GEX file of the default workload: the index built on the
+    device, then random regions (log-uniform 1 kb-10 Mb) fetched one at a time (decode of the members
+    that hold them, records overlapping the region kept); latency percentiles and records/s."""
+    import numpy as np
+    import torch
+
+    from cubam_b200 import bai, serve
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    cfg, n, path, gen_s = ensure_file(args, 0, None)
+    rf = serve.ResidentFile.load(path)
+    torch.cuda.synchronize()
+    bai.build(rf)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    idx = bai.build(rf)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t
+    raw = idx.to_bytes()
+    rng = np.random.default_rng(9)
+    lengths = rf.header.lengths
+    regions = []
+    for _ in range(args.requests):
+        r = int(rng.integers(len(lengths)))
+        size = int(np.exp(rng.uniform(np.log(1e3), np.log(1e7))))
+        beg = int(rng.integers(0, max(int(lengths[r]) - size, 1)))
+        regions.append((r, beg, beg + size))
+    for r, b, e in regions[:10]:
+        bai.fetch(rf, idx, r, b, e)
+    torch.cuda.synchronize()
+    lat, recs = [], 0
+    t0 = time.perf_counter()
+    for r, b, e in regions:
+        t = time.perf_counter()
+        res = bai.fetch(rf, idx, r, b, e)
+        torch.cuda.synchronize()
+        lat.append((time.perf_counter() - t) * 1e3)
+        recs += len(res)
+    span = time.perf_counter() - t0
+    lat = np.array(lat)
+    print(json.dumps({
+        "metric": "BAM region fetch through a BAI index on 1 B200", "value": recs / span, "unit": "records/s",
+        "n_gpus": 1, "steps": len(regions), "warmup": 10, "ms_per_step": span * 1e3 / len(regions),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"{cfg.name}: {n} records; {len(regions)} regions of log-uniform 1 kb-10 Mb, seed 9"},
+        "index": {"build_s": build_s, "bytes": len(raw), "refs": len(idx.refs)},
+        "fetch_ms": {"p50": float(np.percentile(lat, 50)), "p95": float(np.percentile(lat, 95)),
+                     "p99": float(np.percentile(lat, 99))},
+        "records": recs,
+    }), flush=True)
+
+
 def main():
     args = parse()
-    if args.config == "serve":
+    if args.config == "bai":
+        run_bai(args)
+    elif args.config == "serve":
         run_serve(args)
     elif args.config == "uneven":
         run_uneven(args)
