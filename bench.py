@@ -666,6 +666,7 @@ def run_bai(args):
     from cubam_b200 import bai, serve
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    args.config = "gex"
     cfg, n, path, gen_s = ensure_file(args, 0, None)
     rf = serve.ResidentFile.load(path)
     torch.cuda.synchronize()
