@@ -13,8 +13,8 @@ chunks of virtual offsets, and the linear index of the smallest virtual offset p
 - :meth:`BaiIndex.query` gives the chunks to read for a region; :func:`fetch` decodes the members
   that hold them and keeps the records that overlap the region.
 
-Chunks are runs of consecutive records with the same bin; htslib also merges the chunks of a bin
-that touch the same BGZF block, which only makes its index smaller.
+Chunks are runs of consecutive records with the same bin, and two chunks of a bin are merged when
+the first ends in the BGZF block where the second starts (as htslib does, to keep the index small).
 """
 
 from __future__ import annotations
@@ -221,7 +221,13 @@ def build(rf: ResidentFile, decoded: DecodedFile | None = None) -> BaiIndex:
     for s, e in zip(np.concatenate([[0], bounds]), np.concatenate([bounds, [len(run_key)]])):
         if s == e:
             continue
-        refs[int(rk[s])].bins[int(bk[s])] = np.stack([run_u[s:e], run_v[s:e]], axis=1).astype(np.uint64)
+        u, v = run_u[s:e], run_v[s:e]
+        # merge a chunk into the one before when that one ends in the block where it starts
+        new = np.ones(len(u), dtype=bool)
+        new[1:] = (v[:-1] >> 16) < (u[1:] >> 16)
+        mu = u[new]
+        mv = np.maximum.reduceat(v, np.flatnonzero(new))
+        refs[int(rk[s])].bins[int(bk[s])] = np.stack([mu, mv], axis=1).astype(np.uint64)
     for r in range(n_ref):
         R = refs[r]
         if rbeg[r] >= 0:

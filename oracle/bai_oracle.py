@@ -14,8 +14,8 @@ and overlapping bins") with plain Python loops, for small inputs:
 - pseudo-bin 37450 per reference: [first record's offset, end of the last], (mapped, unmapped);
 - records without a reference (ref < 0) are counted in n_no_coor.
 
-Chunks are not merged across runs that touch the same BGZF block (htslib does that to make the
-index smaller; readers accept either).
+Two chunks of a bin are then merged when the first ends in the BGZF block where the second starts
+(the end's block offset at or past the start's), as htslib does to keep the index small.
 """
 
 from __future__ import annotations
@@ -87,6 +87,15 @@ def build(n_ref: int, ref, pos, end, flag, voff, voff_next) -> bytes:
             R["unmapped"] += 1
         else:
             R["mapped"] += 1
+    for R in refs:
+        for b, chunks in R["bins"].items():
+            merged = [chunks[0]]
+            for c in chunks[1:]:
+                if merged[-1][1] >> 16 >= c[0] >> 16:
+                    merged[-1] = [merged[-1][0], max(merged[-1][1], c[1])]
+                else:
+                    merged.append(c)
+            R["bins"][b] = merged
     out = [b"BAI\x01", struct.pack("<i", n_ref)]
     for R in refs:
         bins = sorted(R["bins"].items())
