@@ -308,6 +308,8 @@ def run_ours(args):
     if not args.no_plain:
         plain = plain_per_chunk(comp, header, args.chunk_bytes, tags)
 
+    fused = fused_record_pass(comp, header) if rank == 0 else None
+
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(path, args, tags, inflated, rank, dist)
@@ -365,6 +367,8 @@ def run_ours(args):
     }
     if plain:
         line["plain_per_chunk"] = plain
+    if fused:
+        line["fused_record_pass"] = fused
     if e2e:
         line["e2e"] = e2e
     if cpu:
@@ -374,6 +378,47 @@ def run_ours(args):
         import torch.distributed as td
 
         td.destroy_process_group()
+
+
+def fused_record_pass(comp, header):
+    """Columns + aligned length + read-name hash of all records: three kernels (fixed columns, then the two
+    on-request decoders, each reading the records again) against one fused pass (cb_decode_records)."""
+    import torch
+
+    from cubam_b200 import _lib, batch
+    from cubam_b200.bam import _TYPES, FIELDS
+    from cubam_b200.bgzf import stream_ptr
+
+    d = batch.decode_resident(comp, header, tags=())
+    n = len(d)
+    cols = {k: torch.empty(n, dtype=t, device="cuda") for k, t in _TYPES.items()}
+    al = torch.empty(n, dtype=torch.int32, device="cuda")
+    nh = torch.empty(n, dtype=torch.uint64, device="cuda")
+    ptrs = [cols[k].data_ptr() for k in FIELDS]
+    data, off, s = d.data.data_ptr(), d.offset.data_ptr(), stream_ptr()
+
+    def separate():
+        _lib.lib.cb_decode_fixed(data, off, n, *ptrs, s)
+        _lib.lib.cb_aligned_length(data, off, n, al.data_ptr(), s)
+        _lib.lib.cb_name_hash(data, off, n, nh.data_ptr(), s)
+
+    def fused():
+        _lib.lib.cb_decode_records(data, off, n, *ptrs, al.data_ptr(), nh.data_ptr(), s)
+
+    out = {"records": n}
+    for name, fn in (("separate_ms", separate), ("fused_ms", fused)):
+        fn()
+        times = []
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        out[name] = min(times)
+    del d
+    return out
 
 
 def plain_per_chunk(comp, header, chunk_bytes, tags):

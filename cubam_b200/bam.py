@@ -280,14 +280,30 @@ class RecordBatch:
         self.columns = columns
 
     @classmethod
-    def decode(cls, data: torch.Tensor, offset: torch.Tensor, header: BamHeader) -> RecordBatch:
+    def decode(cls, data: torch.Tensor, offset: torch.Tensor, header: BamHeader, derived: bool = False) -> RecordBatch:
+        """Fixed columns of the records; with ``derived`` also their aligned lengths and read-name hashes,
+        in the same pass over the record bytes (then :meth:`aligned_length` and :meth:`name_hash` return
+        them without reading the records again)."""
         n = int(offset.numel())
         cols = {k: torch.empty(n, dtype=t, device="cuda") for k, t in _TYPES.items()}
+        extra = {}
+        if derived:
+            extra = {"aligned_length": torch.empty(n, dtype=torch.int32, device="cuda"),
+                     "name_hash": torch.empty(n, dtype=torch.uint64, device="cuda")}
         if n:
-            rc = _lib.lib.cb_decode_fixed(data.data_ptr(), offset.data_ptr(), n,
-                                          *(cols[k].data_ptr() for k in FIELDS), stream_ptr())
-            _lib.check(rc, "cb_decode_fixed")
-        return cls(data, offset, header, cols)
+            if derived:
+                rc = _lib.lib.cb_decode_records(data.data_ptr(), offset.data_ptr(), n,
+                                                *(cols[k].data_ptr() for k in FIELDS),
+                                                extra["aligned_length"].data_ptr(), extra["name_hash"].data_ptr(),
+                                                stream_ptr())
+                _lib.check(rc, "cb_decode_records")
+            else:
+                rc = _lib.lib.cb_decode_fixed(data.data_ptr(), offset.data_ptr(), n,
+                                              *(cols[k].data_ptr() for k in FIELDS), stream_ptr())
+                _lib.check(rc, "cb_decode_fixed")
+        b = cls(data, offset, header, cols)
+        b.__dict__["_derived"] = extra
+        return b
 
     def __len__(self) -> int:
         return int(self.offset.numel())
@@ -303,7 +319,11 @@ class RecordBatch:
         idx = torch.as_tensor(idx, device="cuda")
         if idx.dtype == torch.bool:
             idx = torch.nonzero(idx).flatten()
-        return RecordBatch(self.data, self.offset[idx], self.header, {k: _index(v, idx) for k, v in self.columns.items()})
+        b = RecordBatch(self.data, self.offset[idx], self.header, {k: _index(v, idx) for k, v in self.columns.items()})
+        d = self.__dict__.get("_derived")
+        if d:
+            b.__dict__["_derived"] = {k: _index(v, idx) for k, v in d.items()}
+        return b
 
     def record_sizes(self) -> torch.Tensor:
         """Bytes of each record, its length field included (int64)."""
@@ -327,6 +347,9 @@ class RecordBatch:
 
     def name_hash(self) -> torch.Tensor:
         """64-bit FNV-1a hash of the read names (mates share it)."""
+        d = self.__dict__.get("_derived")
+        if d and "name_hash" in d:
+            return d["name_hash"]
         n = len(self)
         out = torch.empty(n, dtype=torch.uint64, device="cuda")
         if n:
@@ -342,6 +365,9 @@ class RecordBatch:
 
     def aligned_length(self) -> torch.Tensor:
         """Number of aligned bases (CIGAR M, = and X) of each read."""
+        d = self.__dict__.get("_derived")
+        if d and "aligned_length" in d:
+            return d["aligned_length"]
         n = len(self)
         out = torch.empty(n, dtype=torch.int32, device="cuda")
         if n:

@@ -86,8 +86,12 @@ class _View:
 
 
 def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "GN"), check_crc: bool = True,
-                events: StageEvents | None = None, counter: dict | None = None) -> list[DecodedFile]:
-    """Decode whole files (compressed bytes on the device) with one inflate launch for all of them."""
+                events: StageEvents | None = None, counter: dict | None = None,
+                derived: bool = False) -> list[DecodedFile]:
+    """Decode whole files (compressed bytes on the device) with one inflate launch for all of them.
+
+    With ``derived`` the columns also hold ``aligned_length`` and ``name_hash``, computed in the
+    same pass over the records as the fixed fields."""
     if events:
         events.mark("start")
     scans = []
@@ -176,11 +180,21 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
         nrec = int(cs.n_records) if int(data.numel()) else 0
         off = offsets[:nrec]
         cols = {k: torch.empty(nrec, dtype=t, device="cuda") for k, t in _TYPES.items()}
+        if derived:
+            cols["aligned_length"] = torch.empty(nrec, dtype=torch.int32, device="cuda")
+            cols["name_hash"] = torch.empty(nrec, dtype=torch.uint64, device="cuda")
         tag_cols = {}
         if nrec:
-            rc = _lib.lib.cb_decode_fixed(data.data_ptr(), off.data_ptr(), nrec, *(cols[k].data_ptr() for k in FIELDS),
-                                          stream_ptr())
-            _lib.check(rc, "cb_decode_fixed")
+            if derived:
+                rc = _lib.lib.cb_decode_records(data.data_ptr(), off.data_ptr(), nrec,
+                                                *(cols[k].data_ptr() for k in FIELDS),
+                                                cols["aligned_length"].data_ptr(), cols["name_hash"].data_ptr(),
+                                                stream_ptr())
+                _lib.check(rc, "cb_decode_records")
+            else:
+                rc = _lib.lib.cb_decode_fixed(data.data_ptr(), off.data_ptr(), nrec,
+                                              *(cols[k].data_ptr() for k in FIELDS), stream_ptr())
+                _lib.check(rc, "cb_decode_fixed")
             if tags:
                 k = len(tags)
                 ty = torch.empty((k, nrec), dtype=torch.uint8, device="cuda")

@@ -13,10 +13,16 @@ __device__ __forceinline__ bool ref_consuming(uint32_t op) {
 
 // ---------------------------------------------------------------- columns
 
+constexpr unsigned long long FNV_OFFSET = 1469598103934665603ULL;
+constexpr unsigned long long FNV_PRIME = 1099511628211ULL;
+
+// The fixed columns (src/cubam/_kernels.py:292-319) and, when their pointers are given, the
+// aligned length and the read-name hash of each record in the same pass over its bytes (the values
+// k_aligned_length and k_name_hash give).
 __global__ void k_decode_fixed(const uint8_t* __restrict__ b, const int64_t* __restrict__ off, long long n,
                                int32_t* ref, int32_t* pos, int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref,
                                int32_t* npos, int32_t* tlen, int32_t* l_seq, uint16_t* clip_left,
-                               uint16_t* clip_right) {
+                               uint16_t* clip_right, int32_t* aligned, uint64_t* name_hash) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long o = off[i];
         const int p = (int)ld_u32(b, o + 8);
@@ -31,10 +37,11 @@ __global__ void k_decode_fixed(const uint8_t* __restrict__ b, const int64_t* __r
         const uint32_t lrn = b[o + 12], ncig = ld_u16(b, o + 16);
         const long long cg = o + 36 + lrn;
         long long rlen = 0;
-        uint32_t cl = 0, cr = 0;
+        uint32_t cl = 0, cr = 0, al = 0;
         for (uint32_t k = 0; k < ncig; k++) {
             uint32_t v = ld_u32(b, cg + 4LL * k), op = v & 15, len = v >> 4;
             if (ref_consuming(op)) rlen += len;
+            if (op == 0 || op == 7 || op == 8) al += len;
             if (op == 4) {
                 if (k == 0) cl = len;
                 else cr = len;
@@ -43,6 +50,15 @@ __global__ void k_decode_fixed(const uint8_t* __restrict__ b, const int64_t* __r
         end[i] = p + (int)rlen;
         clip_left[i] = (uint16_t)(cl > 65535 ? 65535 : cl);
         clip_right[i] = (uint16_t)(cr > 65535 ? 65535 : cr);
+        if (aligned) aligned[i] = (int32_t)al;
+        if (name_hash) {
+            unsigned long long x = FNV_OFFSET;
+            for (uint32_t k = 0; k + 1 < lrn; k++) {
+                x ^= b[o + 36 + k];
+                x *= FNV_PRIME;
+            }
+            name_hash[i] = x;
+        }
     }
 }
 
@@ -122,9 +138,6 @@ __global__ void k_find_tags(const uint8_t* __restrict__ b, const int64_t* __rest
         }
     }
 }
-
-constexpr unsigned long long FNV_OFFSET = 1469598103934665603ULL;
-constexpr unsigned long long FNV_PRIME = 1099511628211ULL;
 
 __global__ void k_name_hash(const uint8_t* __restrict__ b, const int64_t* __restrict__ off, long long n, uint64_t* h) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -349,7 +362,19 @@ extern "C" int cb_decode_fixed(const uint8_t* data, const int64_t* offsets, int6
     if (n < 0) return CB_ERR_ARG;
     if (n == 0) return CB_OK;
     rec::k_decode_fixed<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        data, offsets, n, ref, pos, end, mapq, flag, nref, npos, tlen, l_seq, clip_left, clip_right);
+        data, offsets, n, ref, pos, end, mapq, flag, nref, npos, tlen, l_seq, clip_left, clip_right, nullptr, nullptr);
+    return cb_set_error(cudaGetLastError());
+}
+
+extern "C" int cb_decode_records(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
+                                 int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos,
+                                 int32_t* tlen, int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right,
+                                 int32_t* aligned_length, uint64_t* name_hash, void* stream) {
+    if (n < 0) return CB_ERR_ARG;
+    if (n == 0) return CB_OK;
+    rec::k_decode_fixed<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        data, offsets, n, ref, pos, end, mapq, flag, nref, npos, tlen, l_seq, clip_left, clip_right, aligned_length,
+        name_hash);
     return cb_set_error(cudaGetLastError());
 }
 

@@ -159,6 +159,15 @@ int cb_decode_fixed(const uint8_t* data, const int64_t* offsets, int64_t n, int3
                     int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
                     int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, void* stream);
 
+/* cb_decode_fixed plus, in the same pass over each record, its aligned length (as
+ * cb_aligned_length) and read-name hash (as cb_name_hash), each skipped when its pointer is NULL.
+ * Fuses cubam's on-request decoders aligned_length and name_hash (src/cubam/bam.py:325-332,
+ * src/cubam/bam.py:341-348) into the record pass, so they do not read the records again. */
+int cb_decode_records(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
+                      int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
+                      int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, int32_t* aligned_length,
+                      uint64_t* name_hash, void* stream);
+
 /* ---- Tags: replaces find_tag, one launch per tag (src/cubam/_kernels.py:334-388, src/cubam/bam.py:184-208).
  * One aux walk per record finds k tags (k <= 16); `names` (host) holds 2k characters.  Output is
  * tag-major: type[t * n + i] etc. --------------------------------------------------------------- */

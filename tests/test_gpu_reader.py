@@ -310,3 +310,21 @@ def test_records_cross_members_and_chunks(tmp_path):
             assert _np(g.offset).tolist() == e.offset.tolist()
             for k in O.FIELDS:
                 assert _np(getattr(g, k)).tolist() == e.columns[k].tolist()
+
+
+@pytest.mark.parametrize(("name", "chunk"), [("mixed_b700.bam", 50_000), ("pairs.bam", 1 << 20)])
+def test_fused_record_pass_equals_the_separate_decoders(name, chunk):
+    """decode(derived=True) gives the aligned lengths and name hashes of the separate kernels, in one pass."""
+    from golden_io import GOLDEN
+
+    from cubam_b200.bam import RecordBatch
+
+    for b in cubam_b200.read_bam(GOLDEN / name, chunk_bytes=chunk):
+        f = RecordBatch.decode(b.data, b.offset, b.header, derived=True)
+        for k in b.FIELDS:
+            assert torch.equal(getattr(f, k), getattr(b, k)), k
+        assert torch.equal(f.aligned_length(), b.aligned_length())
+        assert torch.equal(f.name_hash().view(torch.int64), b.name_hash().view(torch.int64))
+        idx = torch.arange(0, len(b), 3, device="cuda")
+        t = f.take(idx)
+        assert torch.equal(t.aligned_length(), b.take(idx).aligned_length())
