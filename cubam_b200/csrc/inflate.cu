@@ -20,6 +20,7 @@
 // per-member errors.
 
 #include "common.cuh"
+#include "crc.cuh"
 
 namespace cb {
 namespace infl {
@@ -52,46 +53,6 @@ __constant__ uint8_t kDistExtra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5,
 // RFC 1951 3.2.7: order of the code length code lengths.
 __constant__ uint8_t kClOrder[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
 
-// ---------------------------------------------------------------- CRC32 arithmetic
-// Reflected representation of GF(2)[x] modulo the CRC-32 polynomial: bit 31 is x^0.
-constexpr uint32_t POLY = 0xEDB88320u;
-
-__host__ __device__ constexpr uint32_t gf_mul(uint32_t a, uint32_t b) {
-    uint32_t p = 0;
-    for (int i = 0; i < 32; i++) {
-        if (a & 0x80000000u) p ^= b;
-        a <<= 1;
-        b = (b & 1u) ? (b >> 1) ^ POLY : (b >> 1);
-    }
-    return p;
-}
-
-struct CrcConst {
-    uint32_t x2n[32];   // x^(2^k)
-    uint32_t seg[5];    // x^(8 * 32 * 2^k): shifts that combine the lane columns
-    uint32_t k992;      // x^(8 * 992): one window minus one column
-};
-
-__host__ __device__ constexpr uint32_t xpow_from(const uint32_t* x2n, unsigned long long n) {
-    uint32_t r = 0x80000000u;  // x^0
-    for (int k = 0; n; n >>= 1, k++)
-        if (n & 1) r = gf_mul(r, x2n[k]);
-    return r;
-}
-
-constexpr CrcConst make_crc_const() {
-    CrcConst c{};
-    uint32_t p = 0x40000000u;  // x^1
-    for (int k = 0; k < 32; k++) {
-        c.x2n[k] = p;
-        p = gf_mul(p, p);
-    }
-    for (int k = 0; k < 5; k++) c.seg[k] = xpow_from(c.x2n, 8ull * 32ull * (1ull << k));
-    c.k992 = xpow_from(c.x2n, 8ull * 992ull);
-    return c;
-}
-
-__constant__ CrcConst kCrc = make_crc_const();
 
 // Slot of x in a ring of RN bytes (x below 2 RN when RN is not a power of two).
 template <uint32_t RN> __device__ __forceinline__ uint32_t slot_of(uint32_t x) {
@@ -987,12 +948,6 @@ __device__ __forceinline__ void ring_store16(uint32_t* ring, uint32_t d, const u
     if (f) ring[(w + 4) & (RW - 1)] = v[3] >> (32 - sh);
 }
 
-__device__ __forceinline__ uint32_t crc_bytes8(const uint32_t (*T)[256], uint32_t c, uint32_t w0, uint32_t w1) {
-    c ^= w0;
-    return T[7][c & 255] ^ T[6][(c >> 8) & 255] ^ T[5][(c >> 16) & 255] ^ T[4][c >> 24] ^ T[3][w1 & 255] ^
-           T[2][(w1 >> 8) & 255] ^ T[1][(w1 >> 16) & 255] ^ T[0][w1 >> 24];
-}
-
 // State of the member a lane inflates.
 struct Lane {
     int st;
@@ -1161,8 +1116,8 @@ __device__ __forceinline__ void ln_flush(Lane& L, const uint32_t* ringw, const t
         const uint4 u = *reinterpret_cast<const uint4*>(ring + ((L.flushed + L.a) & RM));
         *reinterpret_cast<uint4*>(L.out + L.flushed) = u;
         if (crc) {
-            L.crc = crc_bytes8(S.crc8, L.crc, u.x, u.y);
-            L.crc = crc_bytes8(S.crc8, L.crc, u.z, u.w);
+            L.crc = crc_step8(S.crc8, L.crc, u.x, u.y);
+            L.crc = crc_step8(S.crc8, L.crc, u.z, u.w);
         }
         L.flushed += 16;
     }
@@ -1199,22 +1154,6 @@ __device__ __forceinline__ void report(cb_inflate_summary* summary, uint32_t* jo
     }
 }
 
-// Slice-by-8 CRC tables (table t: the CRC of a byte followed by t zero bytes).
-__device__ void init_crc8(uint32_t (*crc8)[256]) {
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        uint32_t c = (uint32_t)i;
-        for (int k = 0; k < 8; k++) c = (c & 1u) ? (c >> 1) ^ POLY : c >> 1;
-        crc8[0][i] = c;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        uint32_t c = crc8[0][i];
-        for (int t = 1; t < 8; t++) {
-            c = (c >> 8) ^ crc8[0][c & 255];
-            crc8[t][i] = c;
-        }
-    }
-}
 
 __global__ void __launch_bounds__(wm::WARPS * 32, 4)
     k_inflate_warp(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
