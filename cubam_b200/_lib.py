@@ -56,6 +56,10 @@ class ChainSummary(ctypes.Structure):
     ]
 
 
+class DeflateSummary(ctypes.Structure):
+    _fields_ = [("total", c_int64), ("n_stored", c_int64), ("status", c_int32), ("reserved", c_int32)]
+
+
 JOB_BYTES = ctypes.sizeof(MemberJob)
 
 P = c_void_p
@@ -86,6 +90,10 @@ _SIGNATURES = {
     "cb_base_at": (c_int, [P, P, P, P, I64, P, P]),
     "cb_copy_spans": (c_int, [P, P, P, P, P, I64, P]),
     "cb_record_sizes": (c_int, [P, P, I64, P, P]),
+    "cb_deflate_workspace_bytes": (c_size_t, [I64]),
+    "cb_deflate_spans": (c_int, [P, P, P, I64, c_int, c_int, P, I64, P, P, P, P, P, c_size_t, P]),
+    "cb_crc32_spans": (c_int, [P, P, P, I64, P, P]),
+    "cb_adler32_spans": (c_int, [P, P, P, I64, P, P]),
 }
 
 

@@ -288,3 +288,13 @@ def _inflate(path: str | Path, chunk_bytes: int | None, prefix, check_crc: bool 
             del data, res
     finally:
         reader.close()
+
+
+# The write side (it imports this module's names, so it comes last).
+from cubam_b200.bgzf_writer import (  # noqa: E402
+    BgzfWriter,
+    _adler32_spans,
+    _bgzf_compress,
+    _crc32_spans,
+    _deflate_spans,
+)

@@ -201,6 +201,45 @@ int cb_copy_spans(const uint8_t* src, uint8_t* dst, const int64_t* src_off, cons
 /* Record sizes incl. the length field (record_sizes, src/cubam/bam.py:308-315). */
 int cb_record_sizes(const uint8_t* data, const int64_t* offsets, int64_t n, int64_t* out, void* stream);
 
+/* ---- BGZF writer: replaces nvcompBatchedDeflateCompressAsync (src/cubam/bgzf.py:292-351, called by
+ * _deflate_spans :248 and _bgzf_compress :380), crc32_spans / adler32_spans
+ * (src/cubam/_kernels.py:93-158) and bgzf_frame (src/cubam/_kernels.py:161-191) ------------------- */
+
+/* Result of cb_deflate_spans (device memory). */
+typedef struct cb_deflate_summary {
+    int64_t total;        /* bytes written to out */
+    int64_t n_stored;     /* spans written as stored blocks (DEFLATE did not shrink them) */
+    int32_t status;       /* CB_OK, CB_ERR_ARG (a span longer than allowed) or CB_ERR_CAPACITY (out too small) */
+    int32_t reserved;
+} cb_deflate_summary;
+
+/* Workspace bytes of cb_deflate_spans for n spans (no device call). */
+size_t cb_deflate_workspace_bytes(int64_t n_spans);
+
+/* Compress the spans data[off[i] : off[i] + size[i]], i < n, each to one raw DEFLATE stream, packed
+ * one after another in out: stream i at out_off[i], out_size[i] bytes (both device arrays of n;
+ * out_size may be NULL).  With bgzf = 0 a span holds at most 65,536 bytes (the reference's limit,
+ * src/cubam/bgzf.py:304); with bgzf = 1 at most 65,280 (BLOCK_DATA) and each stream is framed as a
+ * BGZF member (18-byte header with BSIZE, the stream, CRC32, ISIZE; SAMv1 4.1), so out_size[i] =
+ * stream + 26.  Each span is written as the smallest of a dynamic-Huffman, a fixed-Huffman and a
+ * stored block, so a member always fits BGZF's 64 KiB (the reference's stored fallback,
+ * src/cubam/bgzf.py:401).  level: 0 = Huffman coding only, 1 = greedy matching, 2-9 = matching
+ * with one position of lazy lookahead.  crc (device, n entries, may be NULL) receives the zlib
+ * CRC32 of each span.  out has out_cap bytes; sum(size[i] + 36) always suffices.  Spans must lie
+ * inside one device allocation of data.  summary->total is the number of bytes written; when
+ * summary->status is not CB_OK nothing is written to out.  The output depends only on the input
+ * bytes and the level. */
+int cb_deflate_spans(const uint8_t* data, const int64_t* off, const int64_t* size, int64_t n, int level, int bgzf,
+                     uint8_t* out, int64_t out_cap, int64_t* out_off, int64_t* out_size, uint32_t* crc,
+                     cb_deflate_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
+
+/* zlib CRC32 of each span data[off[i] : off[i] + size[i]] (crc32_spans, src/cubam/_kernels.py:93-141). */
+int cb_crc32_spans(const uint8_t* data, const int64_t* off, const int64_t* size, int64_t n, uint32_t* out,
+                   void* stream);
+/* zlib Adler-32 of each span (adler32_spans, src/cubam/_kernels.py:143-158). */
+int cb_adler32_spans(const uint8_t* data, const int64_t* off, const int64_t* size, int64_t n, uint32_t* out,
+                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif
