@@ -86,17 +86,24 @@ __device__ __forceinline__ uint32_t u32at(const uint32_t* w, uint32_t byte) {
     return __funnelshift_r(w[i], w[i + 1], (byte & 3) * 8);
 }
 
-// Bytes in common at byte offsets q and c (c < q) of the staged span, at most maxl.  Reads at most
-// 7 bytes past q + maxl.
+// 8 bytes at byte offset `byte` of the staged span (three aligned words).
+__device__ __forceinline__ uint64_t u64at(const uint32_t* w, uint32_t byte) {
+    const uint32_t i = byte >> 2, sh = (byte & 3) * 8;
+    const uint32_t w0 = w[i], w1 = w[i + 1], w2 = w[i + 2];
+    return (uint64_t)__funnelshift_r(w0, w1, sh) | ((uint64_t)__funnelshift_r(w1, w2, sh) << 32);
+}
+
+// Bytes in common at byte offsets q and c (c < q) of the staged span, at most maxl, 8 bytes per
+// step.  Reads at most 11 bytes past q + maxl (inside the staging slack).
 __device__ __forceinline__ uint32_t match_len(const uint32_t* w, uint32_t q, uint32_t c, uint32_t maxl) {
     uint32_t L = 0;
     while (L < maxl) {
-        const uint32_t x = u32at(w, q + L) ^ u32at(w, c + L);
+        const uint64_t x = u64at(w, q + L) ^ u64at(w, c + L);
         if (x) {
-            L += (uint32_t)(__ffs(x) - 1) >> 3;
+            L += (uint32_t)(__ffsll((long long)x) - 1) >> 3;
             break;
         }
-        L += 4;
+        L += 8;
     }
     return L < maxl ? L : maxl;
 }
