@@ -50,15 +50,22 @@ constexpr int META = 4;                        // per span: stream bytes, CRC32,
 enum : uint32_t { K_STORED = 0, K_FIXED = 1, K_DYNAMIC = 2 };
 static_assert((1 << LEVELS) == NT, "token m of a tile has LEVELS binary digits");
 
+// Code-length construction of one alphabet (par_lengths).
+struct LenScratch {
+    uint16_t sorted[NLIT_ALL];   // used symbols by ascending (count, symbol)
+    uint32_t A[NLIT_ALL];        // weights, then internal node weights and parent links
+    uint16_t anc[2][NLIT_ALL];   // pointer jumping over internal nodes: ancestor, depth to it
+    uint16_t dep[2][NLIT_ALL];
+    uint32_t c[NLIT_ALL + 2];    // internal nodes per depth
+    uint32_t cum[16];            // codes of length <= l
+    int32_t maxd;
+};
+
 struct HuffScratch {
-    uint16_t lsorted[NLIT_ALL];
-    uint16_t dsorted[32];
-    uint16_t clsorted[20];
-    uint32_t lA[NLIT_ALL];
-    uint32_t dA[32];
-    uint32_t clA[20];
+    LenScratch ls;
     uint8_t rsym[NRLE];
     uint8_t rext[NRLE];
+    uint32_t roff[NRLE];  // bit offset of each code-length symbol within the run-length part
     uint32_t lcode[NLIT_ALL];
     uint32_t dcode[32];
     uint32_t clcode[20];
@@ -76,6 +83,7 @@ struct Smem {
     uint32_t lfreq[NLIT_ALL], dfreq[32], clfreq[20];
     uint8_t llen[NLIT_ALL], dlen[32], cllen[20];
     uint32_t scan[33];
+    uint32_t cnt[3][16], nxt[3][16];  // codes per length and first code per length: literal, distance, code-length
     uint32_t crcw[16], crck[LEVELS];
     int32_t ntok, exitp, nrle, hlit, hdist, hclen, kind, pad_;
     uint32_t hdr_bits, bits;
@@ -131,9 +139,15 @@ __device__ __forceinline__ void rank_symbol(const uint32_t* freq, int nsym, int 
     sorted[r] = (uint16_t)s;
 }
 
+// Per-size constants of span_crc, kept by thread 0 from one span to the next (spans mostly have
+// the same size).
+struct CrcCache {
+    uint32_t seg = 0xFFFFFFFFu, n = 0xFFFFFFFFu, fin = 0;
+};
+
 // The zlib CRC32 of the staged span (bytes a .. a + n of S.in), every thread taking part; the
 // result is valid in thread 0.
-__device__ uint32_t span_crc(Smem& S, uint32_t a, uint32_t n) {
+__device__ uint32_t span_crc(Smem& S, uint32_t a, uint32_t n, CrcCache& cc) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint8_t* in8 = reinterpret_cast<const uint8_t*>(S.in);
     init_crc8(S.u.crc8);
@@ -141,7 +155,8 @@ __device__ uint32_t span_crc(Smem& S, uint32_t a, uint32_t n) {
     // front leave a raw column unchanged), so all columns are seg bytes long
     const uint32_t seg = ((n + NT - 1) / NT + 7) & ~7u;
     const int32_t pad = (int32_t)(NT * seg) - (int32_t)n;
-    if (t == 0) {
+    if (t == 0 && seg != cc.seg) {
+        cc.seg = seg;
         uint32_t c = xpow_from(kCrc.x2n, 8ull * seg);
         for (int k = 0; k < LEVELS; k++) {
             S.crck[k] = c;
@@ -172,7 +187,13 @@ __device__ uint32_t span_crc(Smem& S, uint32_t a, uint32_t n) {
             const uint32_t other = __shfl_down_sync(FULL, v, 1 << (k - 5));
             if ((lane & ((2 << (k - 5)) - 1)) == 0) v = gf_mul(v, S.crck[k]) ^ other;
         }
-        crc = crc_finish(v, n);
+        if (t == 0) {
+            if (n != cc.n) {
+                cc.n = n;
+                cc.fin = gf_mul(0xFFFFFFFFu, xpow_from(kCrc.x2n, 8ull * n));
+            }
+            crc = v ^ cc.fin ^ 0xFFFFFFFFu;  // crc_finish(v, n)
+        }
     }
     return crc;
 }
@@ -257,75 +278,177 @@ __device__ uint32_t tokenize(Smem& S, uint32_t a, uint32_t n, int level, uint32_
     return tbase;
 }
 
-// Code lengths, the block kind and its size, and the codes the emitter uses (threads 0 and 32
-// do the serial parts).
+// Code lengths (at most L bits) of the symbols 0..nrank-1 with counts freq, into len[0..nlen), as
+// build_lengths gives them; every thread takes part.  Thread 0 runs the first, sequential pass of
+// the Moffat-Katajainen method (the merge of leaves and internal nodes); the depths of internal
+// nodes come from pointer jumping over its parent links, the leaves per depth from a histogram of
+// those depths, and each symbol's length from its rank (lengths_from_depths, length_of_rank).
+__device__ void par_lengths(Smem& S, const uint32_t* freq, int nrank, int nlen, uint32_t L, uint8_t* len) {
+    const int t = threadIdx.x;
+    LenScratch& P = S.u.h.ls;
+    if (t < nrank) rank_symbol(freq, nrank, t, P.sorted);
+    const int m = __syncthreads_count(t < nrank && freq[t] != 0);
+    if (t < nlen) len[t] = 0;
+    if (t < m) P.A[t] = freq[P.sorted[t]];
+    for (int i = t; i < m + 2; i += NT) P.c[i] = 0u;
+    if (t == 0) P.maxd = 0;
+    __syncthreads();
+    if (m < 2) {  // a complete two-code all the same, as decoders want
+        if (t == 0) {
+            if (m == 0) {
+                len[0] = len[1] = 1;
+            } else {
+                len[P.sorted[0]] = 1;
+                len[P.sorted[0] == 0 ? 1 : 0] = 1;
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    if (t == 0) mk_pass1(P.A, m);
+    __syncthreads();
+    const int ni = m - 1, root = m - 2;  // internal nodes; the last one is the root
+    if (t < ni) {
+        P.anc[0][t] = (uint16_t)(t == root ? t : P.A[t]);
+        P.dep[0][t] = (uint16_t)(t == root ? 0 : 1);
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int r = 0; r < LEVELS; r++) {  // depths below 2^LEVELS = 512 > NLIT_ALL
+        bool more = false;
+        if (t < ni) {
+            const uint32_t a = P.anc[cur][t];
+            P.dep[cur ^ 1][t] = (uint16_t)(P.dep[cur][t] + P.dep[cur][a]);
+            const uint32_t aa = P.anc[cur][a];
+            P.anc[cur ^ 1][t] = (uint16_t)aa;
+            more = aa != (uint32_t)root;
+        }
+        cur ^= 1;
+        if (!__syncthreads_or(more)) break;
+    }
+    if (t < ni) {
+        atomicAdd(&P.c[P.dep[cur][t]], 1u);
+        atomicMax(&P.maxd, (int)P.dep[cur][t]);
+    }
+    __syncthreads();
+    if (t == 0) lengths_from_depths(P.c, P.maxd, L, P.cum);
+    __syncthreads();
+    if (t < m) len[P.sorted[t]] = (uint8_t)length_of_rank((uint32_t)(m - 1 - t), P.cum);
+    __syncthreads();
+}
+
+// First code of each length (RFC 1951 3.2.2) from the number of codes of each length.
+__device__ __forceinline__ void first_codes(const uint32_t* cnt, uint32_t* nxt) {
+    uint32_t c = 0;
+    nxt[0] = 0;
+    for (int l = 1; l <= 15; l++) {
+        c = (c + (l > 1 ? cnt[l - 1] : 0u)) << 1;
+        nxt[l] = c;
+    }
+}
+
+// The canonical code of symbol s (as canonical_codes): the first code of its length plus the
+// number of earlier symbols of that length; length << 16 | the code's bits reversed.
+__device__ __forceinline__ uint32_t canonical_of(const uint8_t* len, int s, const uint32_t* nxt) {
+    const uint32_t l = len[s];
+    if (!l) return 0u;
+    uint32_t r = 0;
+    for (int j = 0; j < s; j++) r += len[j] == l;
+    return (l << 16) | reverse_bits(nxt[l] + r, l);
+}
+
+// Code lengths, the block kind and its size, and the codes the emitter uses, every thread taking
+// part (the same results as the serial build_lengths, rle_lengths and canonical_codes).
 __device__ void build_codes(Smem& S, uint32_t n) {
     const int t = threadIdx.x;
     HuffScratch& H = S.u.h;
-    if (t < NLIT) rank_symbol(S.lfreq, NLIT, t, H.lsorted);
-    else if (t >= 320 && t < 320 + NDIST) rank_symbol(S.dfreq, NDIST, t - 320, H.dsorted);
-    const int nl = __syncthreads_count(t < NLIT && S.lfreq[t] != 0);
-    const int nd = __syncthreads_count(t < NDIST && S.dfreq[t] != 0);
-    if (t == 0) build_lengths(S.lfreq, H.lsorted, nl, NLIT_ALL, H.lA, S.llen, MAXBITS);
-    if (t == 32) build_lengths(S.dfreq, H.dsorted, nd, NDIST, H.dA, S.dlen, MAXBITS);
-    __syncthreads();
+    par_lengths(S, S.lfreq, NLIT, NLIT_ALL, MAXBITS, S.llen);
+    par_lengths(S, S.dfreq, NDIST, NDIST, MAXBITS, S.dlen);
     if (t == 0) {
-        int hlit = NLIT;
-        while (hlit > 257 && S.llen[hlit - 1] == 0) hlit--;
-        int hdist = NDIST;
-        while (hdist > 1 && S.dlen[hdist - 1] == 0) hdist--;
-        const int nrle = rle_lengths(S.llen, hlit, S.dlen, hdist, H.rsym, H.rext);
-        for (int s = 0; s < NCL; s++) S.clfreq[s] = 0;
-        for (int k = 0; k < nrle; k++) S.clfreq[H.rsym[k]]++;
-        int m = 0;  // insertion sort of the used code-length symbols by (count, symbol)
-        for (int s = 0; s < NCL; s++) {
-            if (!S.clfreq[s]) continue;
-            int j = m++;
-            while (j > 0 && S.clfreq[H.clsorted[j - 1]] > S.clfreq[s]) {
-                H.clsorted[j] = H.clsorted[j - 1];
-                j--;
-            }
-            H.clsorted[j] = (uint16_t)s;
+        S.hlit = 257;
+        S.hdist = 1;
+    }
+    if (t < 20) S.clfreq[t] = 0u;
+    __syncthreads();
+    if (t < NLIT && S.llen[t]) atomicMax(&S.hlit, t + 1);
+    if (t < NDIST && S.dlen[t]) atomicMax(&S.hdist, t + 1);
+    __syncthreads();
+    // run-length coding of the code lengths: each run of equal lengths writes its symbols at the
+    // prefix sum of the symbol counts of the runs before it
+    const int hlit = S.hlit, T = hlit + S.hdist;
+    int cnt = 0, run = 0;
+    uint8_t v = 0;
+    if (t < T) {
+        v = t < hlit ? S.llen[t] : S.dlen[t - hlit];
+        const uint8_t prev = t == 0 ? 0xFF : (t - 1 < hlit ? S.llen[t - 1] : S.dlen[t - 1 - hlit]);
+        if (v != prev) {
+            run = 1;
+            while (t + run < T && (t + run < hlit ? S.llen[t + run] : S.dlen[t + run - hlit]) == v) run++;
+            cnt = rle_run(v, run, nullptr, nullptr);
         }
-        build_lengths(S.clfreq, H.clsorted, m, NCL, H.clA, S.cllen, CLBITS);
+    }
+    uint32_t nrle;
+    const uint32_t ro = block_exclusive_scan<NT>((uint32_t)cnt, nrle, S.scan);
+    if (cnt) {
+        rle_run(v, run, H.rsym + ro, H.rext + ro);
+        for (int k = 0; k < cnt; k++) atomicAdd(&S.clfreq[H.rsym[ro + k]], 1u);
+    }
+    __syncthreads();
+    par_lengths(S, S.clfreq, NCL, NCL, CLBITS, S.cllen);
+    if (t == 0) {
         int hclen = NCL;
         while (hclen > 4 && S.cllen[cl_order(hclen - 1)] == 0) hclen--;
-        uint64_t hdr = 3 + 14 + 3 * (uint64_t)hclen;
-        for (int k = 0; k < nrle; k++) hdr += S.cllen[H.rsym[k]] + cl_extra_bits(H.rsym[k]);
-        uint64_t dyn = hdr, fix = 3;
-        for (int s = 0; s < NLIT; s++) {
-            const uint64_t f = S.lfreq[s];
-            if (!f) continue;
-            const uint32_t e = s > 256 ? len_extra_bits(s) : 0;
-            dyn += f * (S.llen[s] + e);
-            fix += f * (fixed_lit_len(s) + e);
-        }
-        for (int d = 0; d < NDIST; d++) {
-            const uint64_t f = S.dfreq[d];
-            dyn += f * (S.dlen[d] + dist_extra_bits(d));
-            fix += f * (FIXED_DIST_LEN + dist_extra_bits(d));
-        }
+        S.hclen = hclen;
+        S.nrle = (int32_t)nrle;
+    }
+    if (t < 48) S.cnt[t >> 4][t & 15] = 0u;
+    __syncthreads();
+    // bits of the dynamic payload, the fixed payload and the run-length part of the header
+    uint32_t dyn = 0, fix = 0, hdr = 0;
+    if (t < NLIT) {
+        const uint32_t f = S.lfreq[t], e = t > 256 ? len_extra_bits(t) : 0;
+        dyn = f * (S.llen[t] + e);
+        fix = f * (fixed_lit_len(t) + e);
+    } else if (t >= 320 && t < 320 + NDIST) {
+        const uint32_t d = t - 320, f = S.dfreq[d], e = dist_extra_bits(d);
+        dyn = f * (S.dlen[d] + e);
+        fix = f * (FIXED_DIST_LEN + e);
+    }
+    if ((uint32_t)t < nrle) hdr = S.cllen[H.rsym[t]] + cl_extra_bits(H.rsym[t]);
+    uint32_t dyn_t, fix_t, hdr_t;
+    const uint32_t hoff = block_exclusive_scan<NT>(hdr, hdr_t, S.scan);
+    block_exclusive_scan<NT>(dyn, dyn_t, S.scan);
+    block_exclusive_scan<NT>(fix, fix_t, S.scan);
+    if ((uint32_t)t < nrle) H.roff[t] = hoff;
+    if (t == 0) {
+        const uint64_t hdr_bits = 17 + 3 * (uint64_t)S.hclen + hdr_t;
+        const uint64_t dbits = hdr_bits + dyn_t, fbits = 3 + (uint64_t)fix_t;
         const uint64_t nblk = n ? (n + 65534) / 65535 : 1;
         const uint64_t stored = n + 5 * nblk;
-        uint32_t kind = (fix + 7) / 8 <= (dyn + 7) / 8 ? K_FIXED : K_DYNAMIC;
-        const uint64_t bits = kind == K_FIXED ? fix : dyn;
+        uint32_t kind = (fbits + 7) / 8 <= (dbits + 7) / 8 ? K_FIXED : K_DYNAMIC;
+        const uint64_t bits = kind == K_FIXED ? fbits : dbits;
         if (stored < (bits + 7) / 8) kind = K_STORED;
-        if (kind == K_FIXED) {
-            for (int s = 0; s < NLIT_ALL; s++) S.llen[s] = (uint8_t)fixed_lit_len(s);
-            for (int d = 0; d < NDIST; d++) S.dlen[d] = (uint8_t)FIXED_DIST_LEN;
-        }
         S.kind = (int32_t)kind;
         S.bits = (uint32_t)(kind == K_STORED ? stored * 8 : bits);
-        S.hdr_bits = kind == K_DYNAMIC ? (uint32_t)hdr : 3u;
-        S.nrle = nrle;
-        S.hlit = hlit;
-        S.hdist = hdist;
-        S.hclen = hclen;
-        if (kind != K_STORED) canonical_codes(S.llen, NLIT_ALL, H.lcode);
-        if (kind == K_DYNAMIC) canonical_codes(S.cllen, NCL, H.clcode);
+        S.hdr_bits = kind == K_DYNAMIC ? (uint32_t)hdr_bits : 3u;
     }
-    __syncthreads();  // the distance code follows the kind thread 0 picked
-    if (t == 32 && S.kind != (int32_t)K_STORED) canonical_codes(S.dlen, NDIST, H.dcode);
+    __syncthreads();
+    const int kind = S.kind;
+    if (kind == (int32_t)K_STORED) return;
+    if (kind == (int32_t)K_FIXED) {
+        if (t < NLIT_ALL) S.llen[t] = (uint8_t)fixed_lit_len(t);
+        if (t < NDIST) S.dlen[t] = (uint8_t)FIXED_DIST_LEN;
+        __syncthreads();
+    }
+    if (t < NLIT_ALL && S.llen[t]) atomicAdd(&S.cnt[0][S.llen[t]], 1u);
+    if (t >= 320 && t < 320 + NDIST && S.dlen[t - 320]) atomicAdd(&S.cnt[1][S.dlen[t - 320]], 1u);
+    if (t >= 384 && t < 384 + NCL && S.cllen[t - 384]) atomicAdd(&S.cnt[2][S.cllen[t - 384]], 1u);
+    __syncthreads();
+    if (t < 3) first_codes(S.cnt[t], S.nxt[t]);
+    __syncthreads();
+    if (t < NLIT_ALL) H.lcode[t] = canonical_of(S.llen, t, S.nxt[0]);
+    else if (t >= 320 && t < 320 + NDIST) H.dcode[t - 320] = canonical_of(S.dlen, t - 320, S.nxt[1]);
+    else if (t >= 384 && t < 384 + NCL) H.clcode[t - 384] = canonical_of(S.cllen, t - 384, S.nxt[2]);
     __syncthreads();
 }
 
@@ -336,25 +459,20 @@ __device__ void emit(Smem& S, uint32_t ntok, const uint32_t* __restrict__ tok) {
     const uint32_t words = (S.bits + 31) / 32 + 1;
     for (uint32_t w = t; w < words && w < (uint32_t)(INB / 4); w += NT) S.in[w] = 0u;
     __syncthreads();
-    if (t == 0) {
-        uint32_t pos = 0;
-        if (S.kind == (int32_t)K_FIXED) {
-            or_bits(S.in, pos, 1u | (1u << 1), 3);
-        } else {
-            or_bits(S.in, pos, 1u | (2u << 1), 3);
-            or_bits(S.in, pos + 3, (uint32_t)(S.hlit - 257), 5);
-            or_bits(S.in, pos + 8, (uint32_t)(S.hdist - 1), 5);
-            or_bits(S.in, pos + 13, (uint32_t)(S.hclen - 4), 4);
-            pos = 17;
-            for (int i = 0; i < S.hclen; i++, pos += 3) or_bits(S.in, pos, S.cllen[cl_order(i)], 3);
-            for (int k = 0; k < S.nrle; k++) {
-                const uint32_t s = H.rsym[k], c = H.clcode[s];
-                or_bits(S.in, pos, c & 0xFFFFu, c >> 16);
-                pos += c >> 16;
-                const uint32_t e = cl_extra_bits(s);
-                or_bits(S.in, pos, H.rext[k], e);
-                pos += e;
-            }
+    if (S.kind == (int32_t)K_FIXED) {
+        if (t == 0) or_bits(S.in, 0, 1u | (1u << 1), 3);
+    } else {
+        if (t == 0) {
+            or_bits(S.in, 0, 1u | (2u << 1), 3);
+            or_bits(S.in, 3, (uint32_t)(S.hlit - 257), 5);
+            or_bits(S.in, 8, (uint32_t)(S.hdist - 1), 5);
+            or_bits(S.in, 13, (uint32_t)(S.hclen - 4), 4);
+        }
+        if (t < S.hclen) or_bits(S.in, 17 + 3 * t, S.cllen[cl_order(t)], 3);
+        if (t < S.nrle) {
+            const uint32_t s = H.rsym[t], c = H.clcode[s], pos = 17 + 3 * S.hclen + H.roff[t];
+            or_bits(S.in, pos, c & 0xFFFFu, c >> 16);
+            or_bits(S.in, pos + (c >> 16), H.rext[t], cl_extra_bits(s));
         }
     }
     uint32_t base = S.hdr_bits;
@@ -401,6 +519,7 @@ __global__ void __launch_bounds__(NT, 2)
     const int t = threadIdx.x;
     uint8_t* in8 = reinterpret_cast<uint8_t*>(S.in);
     uint32_t* tok = tokens + (int64_t)blockIdx.x * TOKS;
+    CrcCache cc;
     for (int64_t sp = blockIdx.x; sp < n_spans; sp += gridDim.x) {
         const int64_t len = size[sp];
         if (len < 0 || len > max_span) {
@@ -421,7 +540,7 @@ __global__ void __launch_bounds__(NT, 2)
         for (uint32_t c = t; c < nch; c += NT) reinterpret_cast<uint4*>(S.in)[c] = __ldg(g + c);
         __syncthreads();
         if (t < 8 && a + n + t < (uint32_t)INB) in8[a + n + t] = 0;
-        const uint32_t crc = span_crc(S, a, n);
+        const uint32_t crc = span_crc(S, a, n, cc);
         for (int i = t; i < NH; i += NT) S.head[i] = 0u;
         for (int i = t; i < NLIT_ALL; i += NT) S.lfreq[i] = 0u;
         if (t < 32) S.dfreq[t] = 0u;

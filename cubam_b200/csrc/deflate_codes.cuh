@@ -84,9 +84,9 @@ constexpr uint32_t FIXED_DIST_LEN = 5;
 // receives the length of each (A[0], the lightest, gets the longest).  The in-place method of
 // Moffat and Katajainen ("In-place calculation of minimum-redundancy codes", 1995): a first pass
 // forms the internal node weights with parent links, a second turns the links into depths, a
-// third counts leaves per depth.
-__host__ __device__ inline void mk_lengths(uint32_t* A, int m) {
-    // pass 1: A[next] is the weight of internal node next; consumed internal nodes hold their parent
+// third counts leaves per depth.  mk_pass1 is the first pass alone.
+__host__ __device__ inline void mk_pass1(uint32_t* A, int m) {
+    // A[next] becomes the weight of internal node next; consumed internal nodes hold their parent
     int leaf = 2, root = 0;
     A[0] += A[1];
     for (int next = 1; next < m - 1; next++) {
@@ -103,12 +103,16 @@ __host__ __device__ inline void mk_lengths(uint32_t* A, int m) {
             A[next] += A[leaf++];
         }
     }
+}
+
+__host__ __device__ inline void mk_lengths(uint32_t* A, int m) {
+    mk_pass1(A, m);
     // pass 2: depth of each internal node (the root is A[m-2])
     A[m - 2] = 0;
     for (int next = m - 3; next >= 0; next--) A[next] = A[A[next]] + 1;
     // pass 3: leaves per depth, written from the heaviest end
     int avail = 1, used = 0, depth = 0;
-    root = m - 2;
+    int root = m - 2;
     int next = m - 1;
     while (avail > 0) {
         while (root >= 0 && (int)A[root] == depth) {
@@ -149,6 +153,82 @@ __host__ __device__ inline void limit_lengths(uint32_t* A, int m, uint32_t L) {
     int i = 0;
     for (uint32_t l = L; l >= 1; l--)
         for (uint32_t c = bl[l]; c > 0 && i < m; c--) A[i++] = l;
+}
+
+// The same lengths as mk_lengths + limit_lengths, as counts: cum[l] = codes of length <= l
+// (l = 0..L) from c[d] = internal nodes at depth d (d = 0..maxd, the root at depth 0) of the
+// minimum-redundancy tree.  The leaves at depth d are 2 c[d-1] - c[d]; depths over L are limited by
+// the loop of limit_lengths.  The i-th lightest of m symbols then gets length_of_rank(m - 1 - i).
+__host__ __device__ inline void lengths_from_depths(const uint32_t* c, int maxd, uint32_t L, uint32_t* cum) {
+    uint32_t bl[16] = {0};
+    int deepest = 0;
+    for (int d = 1; d <= maxd + 1; d++) {
+        const uint32_t leaves = 2 * c[d - 1] - (d <= maxd ? c[d] : 0u);
+        if (leaves) {
+            deepest = d;
+            bl[d > (int)L ? L : (uint32_t)d] += leaves;
+        }
+    }
+    if (deepest > (int)L) {
+        uint32_t kraft = 0;
+        for (uint32_t l = 1; l <= L; l++) kraft += bl[l] << (L - l);
+        while (kraft > (1u << L) && bl[L] > 0) {
+            bl[L]--;
+            for (uint32_t l = L - 1; l > 0; l--) {
+                if (bl[l]) {
+                    bl[l]--;
+                    bl[l + 1] += 2;
+                    break;
+                }
+            }
+            kraft--;
+        }
+    }
+    cum[0] = 0;
+    for (uint32_t l = 1; l <= L; l++) cum[l] = cum[l - 1] + bl[l];
+    for (uint32_t l = L + 1; l < 16; l++) cum[l] = cum[L];
+}
+
+// The length of the symbol of heavy rank j (0 = the most frequent): the shortest length whose
+// cumulative count passes j.
+__host__ __device__ inline uint32_t length_of_rank(uint32_t j, const uint32_t* cum) {
+    uint32_t l = 1;
+    while (l < 15 && cum[l] <= j) l++;
+    return l;
+}
+
+// The code-length symbols of one run of r >= 1 equal lengths v, as rle_lengths writes them (sym
+// may be null: only counted).  Returns the number of symbols.
+__host__ __device__ inline int rle_run(uint8_t v, int run, uint8_t* sym, uint8_t* ext) {
+    int k = 0;
+    if (v == 0) {
+        while (run >= 11) {
+            const int r = run < 138 ? run : 138;
+            if (sym) { sym[k] = 18; ext[k] = (uint8_t)(r - 11); }
+            k++;
+            run -= r;
+        }
+        if (run >= 3) {
+            if (sym) { sym[k] = 17; ext[k] = (uint8_t)(run - 3); }
+            k++;
+            run = 0;
+        }
+    } else {
+        if (sym) { sym[k] = v; ext[k] = 0; }
+        k++;
+        run--;
+        while (run >= 3) {
+            const int r = run < 6 ? run : 6;
+            if (sym) { sym[k] = 16; ext[k] = (uint8_t)(r - 3); }
+            k++;
+            run -= r;
+        }
+    }
+    for (; run > 0; run--) {
+        if (sym) { sym[k] = v; ext[k] = 0; }
+        k++;
+    }
+    return k;
 }
 
 // Code lengths of an alphabet of nsym symbols from their counts.  sorted[0..m): the symbols with
