@@ -32,8 +32,9 @@ from cubam_b200.bgzf import BLOCK_DATA, EOF_BLOCK, read_struct, stream_ptr
 
 #: Largest span of a raw DEFLATE stream (the reference's limit, ``src/cubam/bgzf.py:304``)
 MAX_DEFLATE_SPAN = 1 << 16
-#: Spans per native call: bounds the workspace (64 KiB of output slot per span)
-SPANS_PER_CALL = 4096
+#: Spans per native call (1 GiB of 64 KiB spans): bounds the workspace, 64 KiB of output slot per
+#: span plus 256 KiB of tokens per resident CTA (about 1.1 GB at this size)
+SPANS_PER_CALL = 16384
 
 
 def _as_index(x, device) -> torch.Tensor:
