@@ -805,6 +805,7 @@ def run_write(args):
         out = _bgzf_compress(data, args.level)
     torch.cuda.synchronize()
     with Clocks(local) as clk:
+        time.sleep(2.0)  # the sampler's start-up, which stalled host syncs of a short timed region
         torch.cuda.synchronize()
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
