@@ -6,11 +6,14 @@ import zlib
 
 import numpy as np
 import pytest
-import torch
-
-from oracle import bgzf_writer_oracle as W
 
 pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from oracle import bgzf_writer_oracle as W  # noqa: E402
 
 
 def dev(b: bytes) -> torch.Tensor:
