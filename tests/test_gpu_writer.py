@@ -156,3 +156,58 @@ def test_round_trip_of_a_bam_through_the_reader(tmp_path):
     b = list(cubam_b200.read_bam(p))
     assert sum(len(x) for x in a) == sum(len(x) for x in b)
     assert torch.cat([x.pos for x in a]).cpu().tolist() == torch.cat([x.pos for x in b]).cpu().tolist()
+
+
+@pytest.fixture(scope="module")
+def host_model(tmp_path_factory):
+    """tests/deflate_model.cu built as a host program: the kernel's DEFLATE coder on one thread."""
+    import subprocess
+    from pathlib import Path
+
+    from cubam_b200 import build
+
+    exe = tmp_path_factory.mktemp("model") / "deflate_model"
+    src = Path(__file__).parent / "deflate_model.cu"
+    subprocess.run([build.nvcc(), "-O2", "-std=c++17", "-Wno-deprecated-gpu-targets", str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    return exe
+
+
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_streams_equal_the_host_model_byte_for_byte(tmp_path, host_model, level):
+    """Every stream of the GPU coder is the host model's, byte for byte (the kernel's parse, codes and
+    block choice are deterministic), on BAM bytes, random bytes, runs and odd span sizes."""
+    import struct
+    import subprocess
+    from pathlib import Path
+
+    from cubam_b200.bgzf import _deflate_spans
+
+    golden = gzip.decompress((Path(__file__).parent / "golden" / "mixed_b65280.bam").read_bytes())
+    rnd = np.random.default_rng(31).integers(0, 256, 70_000, dtype=np.uint8).tobytes()
+    raw = golden + bam_like(600_000, 5) + rnd + b"A" * 70_000 + b"ACGT" * 5_000
+    rng = np.random.default_rng(level)
+    off, size, o = [], [], 0
+    while o < len(raw):
+        n = int(min(len(raw) - o, rng.choice([65_280, 65_536, 1, 3, 4, 511, 512, 513, int(rng.integers(1, 65_536))])))
+        off.append(o)
+        size.append(n)
+        o += n
+    off.append(0)  # an empty span
+    size.append(0)
+    (tmp_path / "in").write_bytes(raw)
+    np.stack([np.array(off, np.int64), np.array(size, np.int64)], 1).tofile(tmp_path / "spans")
+    subprocess.run([str(host_model), str(tmp_path / "in"), str(tmp_path / "spans"), str(level), str(tmp_path / "out")],
+                   check=True)
+    want, p = [], 0
+    blob = (tmp_path / "out").read_bytes()
+    while p < len(blob):
+        n = struct.unpack_from("<I", blob, p)[0]
+        want.append(blob[p + 4 : p + 4 + n])
+        p += 4 + n
+    out, oo, osz = _deflate_spans(dev(raw), off, size, level)
+    got = out.cpu().numpy().tobytes()
+    oo, osz = oo.cpu().tolist(), osz.cpu().tolist()
+    assert len(want) == len(off)
+    for i, (a, b) in enumerate(zip(oo, osz, strict=True)):
+        assert got[a : a + b] == want[i], (i, off[i], size[i])
