@@ -223,7 +223,7 @@ __device__ uint32_t tokenize(Smem& S, uint32_t a, uint32_t n, int level, uint32_
                 const uint32_t L = match_len(S.in, a + p, a + c, maxl);
                 if (L >= MIN_MATCH) best = (L << 16) | (p - c);
             }
-            if (hv) {
+            if (hv && (best >> 16) < maxl) {  // a match of maxl cannot be beaten
                 const uint32_t c = hv - 1;
                 if (p - c <= WSIZE) {
                     const uint32_t L = match_len(S.in, a + p, a + c, maxl);
@@ -476,11 +476,13 @@ __device__ void emit(Smem& S, uint32_t ntok, const uint32_t* __restrict__ tok) {
         }
     }
     uint32_t base = S.hdr_bits;
+    uint32_t next = (uint32_t)t < ntok ? tok[t] : 0u;  // each chunk's tokens are loaded a chunk ahead
     for (uint32_t c0 = 0; c0 < ntok; c0 += NT) {
         const uint32_t i = c0 + t;
+        const uint32_t tk = next;
+        next = i + NT < ntok ? tok[i + NT] : 0u;
         uint32_t v1 = 0, n1 = 0, v2 = 0, n2 = 0;
         if (i < ntok) {
-            const uint32_t tk = tok[i];
             if (tk & 0x80000000u) {
                 const uint32_t L = (tk >> 16) & 0x1FFu, d = (tk & 0xFFFFu) + 1;
                 const uint32_t ls = len_sym(L), lc = H.lcode[ls], lb = lc >> 16;
