@@ -18,10 +18,14 @@ fixed columns and the CB/UB/GN tags.  The metric is GB/s of decompressed
 - ``roofline``: the inflate kernel (the dominant one): decompressed bytes per
   launch / its CUDA-event duration, against the measured HBM copy bandwidth.
 - ``cpu_baseline``: the C oracle (zlib inflate + record chain + columns, all host
-  cores) on a bounded prefix of the same file.
+  cores) on a bounded prefix of the same file; ``parity`` compares the GPU's
+  records, columns and tags of that prefix with the oracle's ("ok" or the first
+  mismatch).
 - ``--impl reference``: cubam's reader needs CuPy, cuDF and nvCOMP and has no
   CPU path; the reference arm times the CPU restatement of its reader path
-  (``oracle/cpu_decoder.c``, all host cores) on the same workload, rank 0 only.
+  (``oracle/cpu_decoder.c``, all host cores) on the whole file of the same
+  workload per step, rank 0 only.  That process loads nothing of ``cubam_b200``:
+  the input file is written by the generator's executable in a child process.
 
 Multi-GPU (torchrun): every rank decodes its own copy of the file (replicas: the
 path shards by file with no exchange), ``scaling`` = weak.
@@ -64,7 +68,7 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="uneven: record counts times this")
     ap.add_argument("--records", type=int, default=None, help="override the workload size (records)")
     ap.add_argument("--chunk-bytes", type=int, default=256 << 20, help="compressed chunk of the e2e read_bam")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-sample-mb", type=int, default=2048, help="compressed MB of the CPU baseline sample")
     ap.add_argument("--workdir", default=None)
     ap.add_argument("--no-e2e", action="store_true")
@@ -99,9 +103,22 @@ def peaks():
     return FALLBACK_HBM, "fallback"
 
 
-def workload(args):
-    from cubam_b200 import synth
+def _synth():
+    """``cubam_b200/synth.py`` loaded on its own: the generator's configurations without importing the
+    package (whose import loads the decoder's library)."""
+    import importlib.util
 
+    mod = sys.modules.get("_cubam_synth")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("_cubam_synth", ROOT / "cubam_b200" / "synth.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_cubam_synth"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(args):
+    synth = _synth()
     cfg = synth.CONFIGS[args.config]
     n = args.records or cfg.n_records
     base = Path(args.workdir or ("/dev/shm" if Path("/dev/shm").exists() else "/tmp"))
@@ -110,14 +127,12 @@ def workload(args):
 
 
 def ensure_file(args, rank, dist):
-    from cubam_b200 import synth
-
     cfg, n, path = workload(args)
     t = 0.0
     if rank == 0 and not path.exists():
         t0 = time.perf_counter()
         tmp = path.with_suffix(f".tmp{os.getpid()}")
-        synth.write_bam(tmp, cfg, n_records=n)
+        _synth().write_bam_process(tmp, cfg, n_records=n)
         tmp.replace(path)
         t = time.perf_counter() - t0
     if dist:
@@ -179,17 +194,21 @@ class Clocks:
 
 
 def cpu_baseline(path: Path, sample_mb: int):
-    """The C oracle on the first ``sample_mb`` MB of compressed members, all host cores."""
+    """The C oracle on the first ``sample_mb`` MB of compressed members, all host cores: the baseline
+    figure and the decoded sample (the checker of the GPU's records)."""
     import numpy as np
 
     from oracle import cpu_oracle
 
     raw = np.fromfile(path, dtype=np.uint8)
     cores = os.cpu_count() or 1
-    cpu_oracle.decode_prefix(raw, sample_mb << 20, cores)  # warm-up: page faults of fresh buffers
-    d = min((cpu_oracle.decode_prefix(raw, sample_mb << 20, cores) for _ in range(2)), key=lambda x: x.seconds["total"])
-    secs = d.seconds["total"]
-    return {
+    ws = {}
+    cpu_oracle.decode_prefix(raw, sample_mb << 20, cores, ws=ws)  # warm-up: page faults of fresh buffers
+    secs, d = None, None
+    for _ in range(2):
+        d = cpu_oracle.decode_prefix(raw, sample_mb << 20, cores, ws=ws)
+        secs = d.seconds["total"] if secs is None else min(secs, d.seconds["total"])
+    return d, {
         "value": d.inflated_bytes / secs / 1e9,
         "unit": UNIT,
         "cores": cores,
@@ -202,7 +221,9 @@ def cpu_baseline(path: Path, sample_mb: int):
 
 
 def run_reference(args):
-    """CPU restatement of the reference's reader path (the reference has no CPU path of its own)."""
+    """CPU restatement of the reference's reader path (the reference has no CPU path of its own): every
+    step decodes the whole file of the workload (all members, records, columns and CB/UB/GN tags) on all
+    host cores.  Nothing of ``cubam_b200`` is imported or loaded in this process."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -213,28 +234,58 @@ def run_reference(args):
 
     raw = np.fromfile(path, dtype=np.uint8)
     cores = os.cpu_count() or 1
-    budget = args.cpu_sample_mb << 20
+    ws = {}  # output arrays kept between steps, so steps do not fault in fresh pages
     for _ in range(args.warmup):
-        cpu_oracle.decode_prefix(raw, min(budget, 64 << 20), cores)
-    times, inflated, recs, members, comp = [], 0, 0, 0, 0
+        cpu_oracle.decode_file(raw, cores, ws=ws)
+    times, inflated, recs, members = [], 0, 0, 0
     for _ in range(args.steps):
-        d = cpu_oracle.decode_prefix(raw, budget, cores)
+        d = cpu_oracle.decode_file(raw, cores, ws=ws)
         times.append(d.seconds["total"])
-        inflated, recs, members, comp = d.inflated_bytes, len(d.offset), d.n_members, d.compressed_bytes
+        inflated, recs, members = d.inflated_bytes, len(d.offset), d.n_members
     ms = statistics.mean(times) * 1e3
     value = inflated / (ms / 1e3) / 1e9
-    sample = (f"first {members} members ({comp / 1e6:.0f} MB compressed, {inflated / 1e6:.0f} MB inflated, "
-              f"{recs} records) of the {cfg.name} workload per step")
+    sample = (f"the whole file per step: {members} members ({raw.size / 1e6:.0f} MB compressed, "
+              f"{inflated / 1e6:.0f} MB of records inflated, {recs} records), zlib inflate + record chain + "
+              f"columns + CB/UB/GN tags")
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
         "config": {"workload": f"{cfg.name}: {n} records, zlib level {cfg.level}, seed {cfg.seed}",
-                   "records_per_step": recs},
+                   "records_per_step": recs, "generate_s": round(gen_s, 1)},
         "records_per_s": recs / (ms / 1e3),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def parity(gpu, ref, tags) -> str:
+    """"ok" when the GPU's decode of a file starts with the oracle's records (offsets, the 11 fixed columns,
+    and type/offset/length/value of each tag), else the first mismatch."""
+    import numpy as np
+
+    from cubam_b200.bam import FIELDS
+
+    n = len(ref.offset)
+    if len(gpu) < n:
+        return f"records: {len(gpu)} on the GPU, {n} in the oracle's sample"
+
+    def first_diff(name, a, b):
+        bad = np.flatnonzero(a != b)
+        return f"{name}: record {int(bad[0])}: GPU {a[bad[0]]}, oracle {b[bad[0]]}" if bad.size else None
+
+    checks = [("offset", gpu.offset[:n], ref.offset)]
+    checks += [(f, gpu.columns[f][:n], ref.columns[f]) for f in FIELDS]
+    for t in tags:
+        g = gpu.tags[t]
+        ty, vo, vl, iv, _ = ref.tags[t]
+        checks += [(f"{t}.type", g.type[:n], ty), (f"{t}.offset", g.offset[:n], vo), (f"{t}.length", g.length[:n], vl),
+                   (f"{t}.value", g.value[:n], iv)]
+    for name, a, b in checks:
+        msg = first_diff(name, a.cpu().numpy(), np.asarray(b))
+        if msg:
+            return msg
+    return "ok"
 
 
 def run_ours(args):
@@ -315,9 +366,13 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(path, args, tags, inflated, rank, dist)
-    cpu = None
+    cpu, checked = None, None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(path, args.cpu_sample_mb)
+        ref, cpu = cpu_baseline(path, args.cpu_sample_mb)
+        res = step()  # one more decode of the whole file, its records checked against the oracle's sample
+        checked = {"result": parity(res, ref, tags), "records": len(ref.offset), "of": n_rec,
+                   "compared": "offsets, 11 fixed columns, CB/UB/GN type/offset/length/value"}
+        del res, ref
     if rank != 0:
         if dist:
             import torch.distributed as td
@@ -375,6 +430,8 @@ def run_ours(args):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    if checked:
+        line["parity"] = checked
     print(json.dumps(line), flush=True)
     if dist:
         import torch.distributed as td

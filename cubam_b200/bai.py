@@ -237,9 +237,11 @@ def build(rf: ResidentFile, decoded: DecodedFile | None = None) -> BaiIndex:
         if len(set_):
             n_intv = int(set_[-1]) + 1
             vals = row[:n_intv].copy()
-            # empty windows take the value of the window before (0 before the first record)
+            # empty windows take the value of the window before; those before the first record's
+            # window take the reference's first record offset (the pseudo-bin's start), as htslib does
             fill = np.maximum.accumulate(np.where(vals >= 0, np.arange(n_intv), -1))
-            R.lin = np.where(fill >= 0, vals[np.maximum(fill, 0)], 0).astype(np.uint64)
+            lead = int(rbeg[r]) if rbeg[r] >= 0 else 0
+            R.lin = np.where(fill >= 0, vals[np.maximum(fill, 0)], lead).astype(np.uint64)
     return BaiIndex(refs, n_no_coor)
 
 

@@ -40,6 +40,23 @@ def build_synth(force: bool = False) -> Path:
     return SYNTH_LIB
 
 
+SYNTH_MAIN = CSRC / "host" / "synth_main.c"
+SYNTH_EXE = OUT_DIR / "cubam_synth"
+
+
+def build_synth_exe(force: bool = False) -> Path:
+    """The generator as an executable (``synth_main.c``): a process of its own writes the file."""
+    newest = max(SYNTH_SRC.stat().st_mtime, SYNTH_MAIN.stat().st_mtime)
+    if not force and SYNTH_EXE.exists() and SYNTH_EXE.stat().st_mtime > newest:
+        return SYNTH_EXE
+    OUT_DIR.mkdir(exist_ok=True)
+    tmp = OUT_DIR / f".cubam_synth.{os.getpid()}"
+    cmd = ["gcc", "-O3", "-pthread", str(SYNTH_SRC), str(SYNTH_MAIN), "-o", str(tmp), "-lz", "-lm"]
+    subprocess.run(cmd, check=True)
+    tmp.replace(SYNTH_EXE)
+    return SYNTH_EXE
+
+
 def _sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [HEADER]
 
@@ -83,3 +100,4 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
     print(build_synth(force="--force" in sys.argv))
+    print(build_synth_exe(force="--force" in sys.argv))

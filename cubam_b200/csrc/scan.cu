@@ -12,6 +12,8 @@
 //     otherwise a walk), applies the reference's checks in the reference's order and writes the
 //     inflate jobs of the non-empty members with their output offsets (prefix sum of ISIZE).
 
+#include <atomic>
+
 #include "common.cuh"
 
 namespace cb {
@@ -326,7 +328,11 @@ constexpr size_t NOALLOC_SCRATCH_BYTES =
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-static void* g_noalloc_ptr[64];  // the array's device address, per device, looked up on first use
+// The array's device address, per device, looked up on the first call on that device.  Atomic, so
+// that host threads calling at once on one device agree (each stores the same address).  The address
+// belongs to the device's primary context: after cudaDeviceReset it is stale, which the header
+// states as unsupported.
+static std::atomic<void*> g_noalloc_ptr[64];
 
 }  // namespace scan
 }  // namespace cb
@@ -343,12 +349,11 @@ extern "C" int cb_scan_members_noalloc(const uint8_t* buf, int64_t n, int eof, i
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cb_set_error(e);
     if (dev < 0 || dev >= 64) return cb_set_error_text(CB_ERR_ARG, "cb_scan_members_noalloc: device index >= 64");
-    if (!scan::g_noalloc_ptr[dev]) {
-        void* p = nullptr;
+    void* p = scan::g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
         e = cudaGetSymbolAddress(&p, scan::g_noalloc_scratch);
         if (e != cudaSuccess) return cb_set_error(e);
-        scan::g_noalloc_ptr[dev] = p;
+        scan::g_noalloc_ptr[dev].store(p, std::memory_order_release);
     }
-    return cb_scan_members(buf, n, eof, out_base_off, jobs, cap, summary, scan::g_noalloc_ptr[dev],
-                           scan::NOALLOC_SCRATCH_BYTES, stream);
+    return cb_scan_members(buf, n, eof, out_base_off, jobs, cap, summary, p, scan::NOALLOC_SCRATCH_BYTES, stream);
 }

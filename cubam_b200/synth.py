@@ -11,20 +11,35 @@ benchmark workloads:
   2% stored members (seed 3), see :func:`uneven_files`.
 
 ``n_records`` overrides the size (tests use small versions of the same shapes).
+:func:`write_bam_process` writes the same file from the generator's executable in a
+child process, so that the caller maps none of this package's libraries.  The
+module imports nothing of the package at load time: a benchmark process that must
+stay free of the decoder can load this file on its own.
 """
 
 from __future__ import annotations
 
 import ctypes
+import importlib.util
 import math
 import os
 import random
+import subprocess
 from dataclasses import dataclass, replace
 from pathlib import Path
 
-from cubam_b200 import build as _build
-
 _lib = None
+_builder = None
+
+
+def _build():
+    """``build.py`` beside this file, loaded on its own (it imports nothing of the package)."""
+    global _builder
+    if _builder is None:
+        spec = importlib.util.spec_from_file_location("_cubam_b200_build_synth", Path(__file__).with_name("build.py"))
+        _builder = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(_builder)
+    return _builder
 
 
 @dataclass(frozen=True)
@@ -48,7 +63,7 @@ CONFIGS = {
 def lib():
     global _lib
     if _lib is None:
-        _lib = ctypes.CDLL(str(_build.build_synth()))
+        _lib = ctypes.CDLL(str(_build().build_synth()))
         _lib.synth_bam.restype = ctypes.c_int
         _lib.synth_bam.argtypes = [
             ctypes.c_char_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_int, ctypes.c_double,
@@ -82,6 +97,22 @@ def write_bam(path: str | Path, config: Config | str, n_records: int | None = No
     if rc:
         raise OSError(f"cannot write {path}")
     return Written(Path(path), cfg, rb.value, mb.value, fb.value)
+
+
+def write_bam_process(path: str | Path, config: Config | str, n_records: int | None = None,
+                      n_threads: int | None = None) -> Written:
+    """:func:`write_bam` run by the generator's executable in a child process (same bytes)."""
+    cfg = CONFIGS[config] if isinstance(config, str) else config
+    if n_records is not None:
+        cfg = replace(cfg, n_records=int(n_records))
+    exe = _build().build_synth_exe()
+    args = [str(exe), str(path), str(cfg.shape), str(cfg.n_records), str(cfg.seed), str(cfg.level),
+            repr(float(cfg.stored_frac)), str(cfg.n_barcodes), str(n_threads or os.cpu_count() or 1)]
+    res = subprocess.run(args, capture_output=True, text=True)
+    if res.returncode:
+        raise OSError(f"cannot write {path}: {res.stderr.strip()}")
+    rb, mb, fb = (int(x) for x in res.stdout.split())
+    return Written(Path(path), cfg, rb, mb, fb)
 
 
 def uneven_files(scale: float = 1.0, seed: int = 3) -> list[Config]:

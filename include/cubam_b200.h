@@ -107,7 +107,9 @@ int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t out_base_off
  * which loads the library holds until the process exits; larger inputs get CB_ERR_CAPACITY (and
  * cb_last_error() says why) before anything is launched.  The caller still passes the input, the
  * job table and the summary.  The first call on a device looks the array's address up for that
- * device (cudaGetSymbolAddress), so make the first call before any stream capture.  All calls share
+ * device (cudaGetSymbolAddress), so make the first call before any stream capture; that address is
+ * kept for the life of the process, so a cudaDeviceReset of a device that has used this entry point
+ * is not supported (later calls would use a stale address).  All calls share
  * the one array: calls that overlap on the GPU (other streams, other threads) race on it and must
  * be serialised by the caller; nothing in it needs to start at zero. */
 #define CB_NOALLOC_SCAN_MAX_BYTES (16LL << 20)

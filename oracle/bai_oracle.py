@@ -10,7 +10,9 @@ and overlapping bins") with plain Python loops, for small inputs:
 - chunks of a bin = runs of consecutive records (file order) with the same bin, as
   [virtual offset of the first record, virtual offset just past the last);
 - linear index = per 16 kb window the smallest virtual offset of a record overlapping it,
-  empty windows taking the value of the window before;
+  empty windows taking the value of the window before, and empty windows before the first
+  record's window the reference's first record offset (the pseudo-bin's start), as htslib
+  fills them;
 - pseudo-bin 37450 per reference: [first record's offset, end of the last], (mapped, unmapped);
 - records without a reference (ref < 0) are counted in n_no_coor.
 
@@ -110,7 +112,7 @@ def build(n_ref: int, ref, pos, end, flag, voff, voff_next) -> bytes:
             out.append(struct.pack("<QQQQ", R["beg"], R["last"], R["mapped"], R["unmapped"]))
         if R["lin"]:
             n_intv = max(R["lin"]) + 1
-            lin, prev = [], 0
+            lin, prev = [], R["beg"] if R["beg"] is not None else 0
             for w in range(n_intv):
                 prev = R["lin"].get(w, prev)
                 lin.append(prev)

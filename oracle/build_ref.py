@@ -1,7 +1,8 @@
 """Build ``oracle/_ref/libref_kernels.so``: the reference's reader kernels compiled for the CPU.
 
 TEST INFRASTRUCTURE ONLY.  Reads ``src/cubam/_kernels.py`` of the reference
-checkout (default ``/root/reference``, or ``$CUBAM_REFERENCE``), takes its
+checkout (``$CUBAM_REFERENCE``, else a directory ``reference`` beside this
+repository's root), takes its
 ``SOURCE`` string unchanged into ``oracle/_ref/ref_kernels.inc`` and compiles it
 with ``oracle/ref_shim.cpp``.  Everything it writes stays under ``oracle/_ref/``
 (git-ignored).  Without a reference checkout it does nothing.
@@ -20,7 +21,9 @@ OUT = HERE / "_ref"
 
 
 def reference_root() -> Path:
-    return Path(os.environ.get("CUBAM_REFERENCE", "/root/reference"))
+    """The reference checkout: ``$CUBAM_REFERENCE``, else ``reference`` next to this repository."""
+    env = os.environ.get("CUBAM_REFERENCE")
+    return Path(env) if env else HERE.parent.parent / "reference"
 
 
 def build(force: bool = False) -> Path | None:

@@ -61,21 +61,35 @@ _DT = dict(ref=np.int32, pos=np.int32, end=np.int32, mapq=np.uint8, flag=np.uint
            tlen=np.int32, l_seq=np.int32, clip_left=np.uint16, clip_right=np.uint16)
 
 
+def _buf(ws: dict | None, name: str, n: int, dtype, shape=None) -> np.ndarray:
+    """An array of ``n`` elements, taken from (and kept in) the workspace ``ws`` when one is given, so that
+    repeated decodes of the same file do not fault in fresh pages every time."""
+    shape = shape or (n,)
+    size = int(np.prod(shape))
+    if ws is None:
+        return np.empty(shape, dtype)
+    a = ws.get(name)
+    if a is None or a.dtype != np.dtype(dtype) or a.size < size:
+        a = np.empty(size, dtype)
+        ws[name] = a
+    return a[:size].reshape(shape)
+
+
 def inflate_file(raw: bytes | np.ndarray, n_threads: int | None = None, check_crc: bool = True,
-                 prefix_bytes: int | None = None):
+                 prefix_bytes: int | None = None, ws: dict | None = None):
     """``(inflated uint8 array, n_members, compressed bytes used)`` of a whole BGZF file, or of the
     members within its first ``prefix_bytes`` bytes."""
     L = lib()
     f = np.frombuffer(raw, np.uint8) if not isinstance(raw, np.ndarray) else raw
     n = f.size if prefix_bytes is None else min(f.size, int(prefix_bytes))
     cap = n // 26 + 2
-    off, bs, isz, oo = (np.empty(cap, np.int64) for _ in range(4))
+    off, bs, isz, oo = (_buf(ws, k, cap, np.int64) for k in ("m_off", "m_bs", "m_isz", "m_oo"))
     m = L.orc_scan_file(_p(f), n, _p(off), _p(bs), _p(isz), _p(oo), cap, int(prefix_bytes is not None))
     if m < 0:
         raise ValueError(f"BGZF scan failed (status {-m})")
     total = int(oo[m - 1] + isz[m - 1]) if m else 0
     used = int(off[m - 1] + bs[m - 1]) if m else 0
-    out = np.empty(max(total, 1), np.uint8)
+    out = _buf(ws, "inflated", max(total, 1), np.uint8)
     st = L.orc_inflate(_p(f), _p(off), _p(bs), _p(isz), _p(oo), m, _p(out), n_threads or os.cpu_count(),
                        int(check_crc))
     if st:
@@ -84,17 +98,18 @@ def inflate_file(raw: bytes | np.ndarray, n_threads: int | None = None, check_cr
 
 
 def decode_file(raw: bytes, n_threads: int | None = None, tags=("CB", "UB", "GN"), check_crc: bool = True,
-                prefix_bytes: int | None = None) -> Decoded:
-    """All records of a BAM file (or of its first ``prefix_bytes`` compressed bytes), on ``n_threads`` threads."""
+                prefix_bytes: int | None = None, ws: dict | None = None) -> Decoded:
+    """All records of a BAM file (or of its first ``prefix_bytes`` compressed bytes), on ``n_threads`` threads.
+    ``ws``: a dict that keeps the output arrays between calls (the results then share its memory)."""
     L = lib()
     nt = n_threads or os.cpu_count()
     t0 = time.perf_counter()
-    data, m, used = inflate_file(raw, nt, check_crc, prefix_bytes)
+    data, m, used = inflate_file(raw, nt, check_crc, prefix_bytes, ws)
     t1 = time.perf_counter()
     _, names, _, skip = read_header(bytes(raw[: min(len(raw), 1 << 20)]) if len(raw) > (1 << 20) else raw)
     data = data[skip:]  # offsets are relative to the records area, as in cubam's batches
     cap = max(data.size // 37 + 2, 1)
-    off = np.empty(cap, np.int64)
+    off = _buf(ws, "offset", cap, np.int64)
     tail = c_int64(0)
     nrec = L.orc_record_chain(_p(data), data.size, 0, len(names), _p(off), cap, ctypes.byref(tail))
     if nrec < 0:
@@ -103,14 +118,14 @@ def decode_file(raw: bytes, n_threads: int | None = None, tags=("CB", "UB", "GN"
         raise ValueError("truncated BAM file (incomplete record at the end)")
     off = off[:nrec]
     t2 = time.perf_counter()
-    cols = {k: np.empty(nrec, t) for k, t in _DT.items()}
-    nh = np.empty(nrec, np.uint64)
+    cols = {k: _buf(ws, "col_" + k, nrec, t) for k, t in _DT.items()}
+    nh = _buf(ws, "name_hash", nrec, np.uint64)
     k = len(tags)
-    ty = np.empty((k, nrec), np.uint8)
-    vo = np.empty((k, nrec), np.int64)
-    vl = np.empty((k, nrec), np.int32)
-    iv = np.empty((k, nrec), np.int64)
-    th = np.empty((k, nrec), np.uint64)
+    ty = _buf(ws, "tag_type", 0, np.uint8, (k, nrec))
+    vo = _buf(ws, "tag_offset", 0, np.int64, (k, nrec))
+    vl = _buf(ws, "tag_length", 0, np.int32, (k, nrec))
+    iv = _buf(ws, "tag_value", 0, np.int64, (k, nrec))
+    th = _buf(ws, "tag_hash", 0, np.uint64, (k, nrec))
     L.orc_decode(_p(data), _p(off), nrec, nt, *(_p(cols[f]) for f in FIELDS), _p(nh), k, "".join(tags).encode(),
                  _p(ty), _p(vo), _p(vl), _p(iv), _p(th))
     t3 = time.perf_counter()
@@ -121,6 +136,7 @@ def decode_file(raw: bytes, n_threads: int | None = None, tags=("CB", "UB", "GN"
     return d
 
 
-def decode_prefix(raw, prefix_bytes: int, n_threads: int | None = None, tags=("CB", "UB", "GN")) -> Decoded:
+def decode_prefix(raw, prefix_bytes: int, n_threads: int | None = None, tags=("CB", "UB", "GN"),
+                  ws: dict | None = None) -> Decoded:
     """The members within the first ``prefix_bytes`` bytes of a BAM file (a bounded CPU sample)."""
-    return decode_file(raw, n_threads, tags, True, prefix_bytes)
+    return decode_file(raw, n_threads, tags, True, prefix_bytes, ws)

@@ -1,7 +1,8 @@
 """Write the golden vectors under ``tests/golden/`` from the reference itself.
 
-Run here, where the reference checkout exists (``/root/reference`` or
-``$CUBAM_REFERENCE``):  ``python tests/golden/make_golden.py``.
+Run where the reference checkout exists (``$CUBAM_REFERENCE``, else a
+directory ``reference`` beside this repository's root):
+``python tests/golden/make_golden.py``.
 
 1. The BAM/BGZF inputs are written by the reference's own fixture writer,
    ``tests/bamwriter.py`` (zlib level 6 raw deflate, ``bamwriter.py:15-29``),

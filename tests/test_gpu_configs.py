@@ -1,0 +1,106 @@
+"""GPU parity on the benchmark workloads themselves, against the C oracle.
+
+- the small workload exactly as specified (100,000 single-end 90 bp records, one 1 Mb reference,
+  uniform qualities 2..41, CB from 1,000 barcodes, UB random; seed 0), read by ``read_bam`` at
+  three chunk sizes that split records across members and chunks: every batch's record bytes,
+  offsets, the 11 fixed columns, the CB/UB tags, their FNV-1a hashes and packed codes, and the
+  read-name hashes;
+- GEX- and ATAC-shaped files of 1,000,000 records (the shapes of the 50M-record and 100M-record
+  workloads, fewer records), read by ``read_bam`` in 32 MB chunks and by the batched whole-file
+  decoder: columns and CB/UB/GN tags.
+
+The oracle is ``oracle/cpu_decoder.c`` (zlib inflate, record chain, columns, tags on the host).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+import cubam_b200  # noqa: E402
+from cubam_b200 import batch, synth  # noqa: E402
+from oracle import bam_oracle as O  # noqa: E402
+from oracle import cpu_oracle  # noqa: E402
+
+FIELDS = cubam_b200.RecordBatch.FIELDS
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def small(tmp_path_factory):
+    path = tmp_path_factory.mktemp("cfg") / "small.bam"
+    synth.write_bam(path, "small")
+    raw = path.read_bytes()
+    return path, cpu_oracle.decode_file(raw, tags=("CB", "UB"))
+
+
+def _check_batches(batches, ref, tags, packed=False):
+    """The batches of ``read_bam``, in order, equal the oracle's decode of the whole file."""
+    k = 0
+    for b in batches:
+        n = len(b)
+        off = _np(b.offset)
+        roff = ref.offset[k : k + n]
+        # the same records: positions relative to the batch's first record, and the record bytes
+        assert (off - off[0]).tolist() == (roff - roff[0]).tolist()
+        end = int(roff[-1]) + int(np.frombuffer(ref.data[int(roff[-1]) : int(roff[-1]) + 4], "<u4")[0]) + 4
+        assert _np(b.data[int(off[0]) : int(off[0]) + end - int(roff[0])]).tobytes() == ref.data[int(roff[0]) : end].tobytes()
+        for f in FIELDS:
+            assert _np(getattr(b, f)).tolist() == ref.columns[f][k : k + n].tolist(), f
+        assert _np(b.name_hash()).tolist() == ref.name_hash[k : k + n].tolist()
+        for name, t in zip(tags, b.tags(*tags)):
+            ty, vo, vl, iv, th = (x[k : k + n] for x in ref.tags[name])
+            assert _np(t.type).tolist() == ty.tolist(), name
+            assert (_np(t.offset) - off).tolist() == (vo - roff).tolist(), name  # offset within the record
+            assert _np(t.length).tolist() == vl.tolist(), name
+            assert _np(t.value).tolist() == iv.tolist(), name
+            assert _np(t.hash()).tolist() == th.tolist(), name
+            if packed:
+                codes, ok = t.packed()
+                ecodes, eok = O.tag_packed(ref.data.tobytes(), ty, vo, vl)
+                assert _np(codes).tolist() == np.asarray(ecodes).tolist(), name
+                assert _np(ok).tolist() == np.asarray(eok, dtype=bool).tolist(), name
+        k += n
+    assert k == len(ref.offset)
+
+
+@pytest.mark.parametrize("chunk", [1 << 20, 3_000_017, 64 << 20])
+def test_small_workload_read_bam(small, chunk):
+    path, ref = small
+    assert len(ref.offset) == 100_000
+    _check_batches(cubam_b200.read_bam(path, chunk_bytes=chunk), ref, ("CB", "UB"), packed=True)
+
+
+@pytest.fixture(scope="module", params=["gex", "atac"])
+def shaped(request, tmp_path_factory):
+    path = tmp_path_factory.mktemp("cfg") / f"{request.param}_1m.bam"
+    synth.write_bam(path, request.param, n_records=1_000_000)
+    return path, cpu_oracle.decode_file(path.read_bytes(), tags=("CB", "UB", "GN"))
+
+
+def test_shaped_workloads_read_bam(shaped):
+    path, ref = shaped
+    assert len(ref.offset) == 1_000_000
+    _check_batches(cubam_b200.read_bam(path, chunk_bytes=32 << 20), ref, ("CB", "UB", "GN"))
+
+
+def test_shaped_workloads_batched(shaped):
+    path, ref = shaped
+    comp = batch.load_compressed(path)
+    d = batch.decode_resident(comp, cubam_b200.BamHeader.read(path), tags=("CB", "UB", "GN"))
+    assert _np(d.offset).tolist() == ref.offset.tolist()
+    for f in FIELDS:
+        assert _np(d.columns[f]).tolist() == ref.columns[f].tolist(), f
+    for name, t in d.tags.items():
+        ty, vo, vl, iv, _ = ref.tags[name]
+        assert _np(t.type).tolist() == ty.tolist(), name
+        assert _np(t.offset).tolist() == vo.tolist(), name
+        assert _np(t.length).tolist() == vl.tolist(), name
+        assert _np(t.value).tolist() == iv.tolist(), name
