@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import gzip
 import struct
+import zlib
 from collections.abc import Iterator
 from dataclasses import dataclass
 from pathlib import Path
@@ -63,9 +64,69 @@ def _ptr(t: torch.Tensor | None):
     return None if t is None or t.numel() == 0 else t.data_ptr()
 
 
+class _MemberStream:
+    """The inflated bytes of a gzip/BGZF file, produced member by member as a reader asks for them.
+
+    Only as many members are read and inflated as the bytes asked for need: a BAM header takes the
+    first member or few of a file of any size.  A file that is not gzip raises
+    :class:`gzip.BadGzipFile`, as reading it with :mod:`gzip` would.
+    """
+
+    _READ = 1 << 16
+
+    def __init__(self, path: str | Path):
+        self._fh = open(path, "rb")  # noqa: SIM115  (closed by close())
+        self._inflater = zlib.decompressobj(31)  # a gzip member: header, raw DEFLATE, trailer
+        self._have = bytearray()
+        self._raw = b""  # file bytes read but not yet given to the inflater
+        self._started = False
+        self._spent = False  # the file has no more bytes
+
+    def close(self) -> None:
+        self._fh.close()
+
+    def _more(self) -> bool:
+        """Inflate some more of the file into the buffer; False once nothing is left."""
+        while True:
+            raw, self._raw = self._raw, b""
+            if not raw:
+                if self._spent:
+                    return False
+                raw = self._fh.read(self._READ)
+                if not raw:
+                    self._spent = True
+                    return False
+            try:
+                got = self._inflater.decompress(raw)
+            except zlib.error as e:
+                if not self._started:
+                    raise gzip.BadGzipFile(f"Not a gzipped file ({raw[:2]!r})") from e
+                raise
+            self._started = True
+            self._have += got
+            if self._inflater.eof:  # the member ended: what is left of raw starts the next one
+                self._raw = self._inflater.unused_data
+                self._inflater = zlib.decompressobj(31)
+            if got:
+                return True
+
+    def take(self, n: int) -> bytes | None:
+        """The next ``n`` inflated bytes, or None when the file ends first (or ``n`` is negative)."""
+        if n < 0:
+            return None
+        while len(self._have) < n:
+            if not self._more():
+                return None
+        out = bytes(self._have[:n])
+        del self._have[:n]
+        return out
+
+
 @dataclass(frozen=True)
 class BamHeader:
-    """The header of a BAM file: SAM text, references, and where the records start (``bam.py:40-100``)."""
+    """The header of a BAM file: SAM text, reference names and lengths, and ``size``, the inflated
+    bytes before the first record (the API of cubam's ``BamHeader``, ``src/cubam/bam.py:40-100``,
+    with its error messages)."""
 
     text: str
     names: list[str]
@@ -74,54 +135,67 @@ class BamHeader:
 
     @classmethod
     def read(cls, path: str | Path) -> BamHeader:
-        with gzip.open(path, "rb") as fh:
+        """Parse the header at the start of a BAM file; only the members that hold it are inflated."""
+        src = _MemberStream(path)
+        try:
+            return cls._parse(src, str(path))
+        finally:
+            src.close()
 
-            def take(n: int) -> bytes:
-                b = fh.read(n)
-                if len(b) != n:
-                    raise ValueError(f"{path}: truncated BAM header")
-                return b
+    @classmethod
+    def _parse(cls, src: _MemberStream, where: str) -> BamHeader:
+        def need(n: int) -> bytes:
+            got = src.take(n)
+            if got is None:
+                raise ValueError(f"{where}: truncated BAM header")
+            return got
 
-            if take(4) != b"BAM\1":
-                raise ValueError(f"{path}: not a BAM file")
-            (l_text,) = struct.unpack("<i", take(4))
-            text = take(l_text).split(b"\0", 1)[0].decode()
-            (n_ref,) = struct.unpack("<i", take(4))
-            names, lengths = [], []
-            size = 12 + l_text
-            for _ in range(n_ref):
-                (ln,) = struct.unpack("<i", take(4))
-                names.append(take(ln)[:-1].decode())
-                (lr,) = struct.unpack("<i", take(4))
-                lengths.append(lr)
-                size += 8 + ln
+        def i32() -> int:
+            return struct.unpack("<i", need(4))[0]
+
+        if need(4) != b"BAM\1":
+            raise ValueError(f"{where}: not a BAM file")
+        l_text = i32()
+        sam = need(l_text)
+        nul = sam.find(b"\0")
+        text = (sam if nul < 0 else sam[:nul]).decode()
+        n_ref = i32()
+        names, lengths, size = [], [], 12 + l_text
+        for _ in range(max(n_ref, 0)):
+            l_name = i32()
+            names.append(need(l_name)[:-1].decode())  # the name without its terminating byte
+            lengths.append(i32())
+            size += 8 + l_name
         return cls(text, names, lengths, size)
+
+    def _hd_fields(self) -> list[str]:
+        hd = self.text.partition("\n")[0]
+        return hd.split("\t")[1:] if hd.startswith("@HD") else []
 
     @property
     def sort_order(self) -> str:
         """``SO`` of the ``@HD`` line (``unknown`` without one)."""
-        first = self.text.split("\n", 1)[0]
-        if first.startswith("@HD"):
-            for field in first.split("\t")[1:]:
-                if field.startswith("SO:"):
-                    return field[3:]
-        return "unknown"
+        return next((f[3:] for f in self._hd_fields() if f.startswith("SO:")), "unknown")
 
     def to_bytes(self, text: str | None = None) -> bytes:
         """The uncompressed BAM header, with ``text`` in place of the SAM text."""
-        t = (self.text if text is None else text).encode()
-        out = [b"BAM\1", struct.pack("<i", len(t)), t, struct.pack("<i", len(self.names))]
+        sam = (self.text if text is None else text).encode()
+        refs = bytearray()
         for name, length in zip(self.names, self.lengths, strict=True):
-            nb = name.encode() + b"\0"
-            out += [struct.pack("<i", len(nb)), nb, struct.pack("<i", length)]
-        return b"".join(out)
+            nb = name.encode()
+            refs += struct.pack("<i", len(nb) + 1) + nb + b"\0" + struct.pack("<i", length)
+        return b"BAM\1" + struct.pack("<i", len(sam)) + sam + struct.pack("<i", len(self.names)) + bytes(refs)
 
     def require_coordinate_sorted(self, path: str | Path = "BAM") -> None:
-        if self.sort_order != "coordinate":
-            raise ValueError(f"{path}: not coordinate-sorted (@HD SO:{self.sort_order})")
+        """ValueError unless ``@HD SO`` is ``coordinate``."""
+        order = self.sort_order
+        if order != "coordinate":
+            raise ValueError(f"{path}: not coordinate-sorted (@HD SO:{order})")
 
     def lines(self, kind: str) -> list[str]:
-        return [line for line in self.text.split("\n") if line.startswith(kind + "\t")]
+        """The header lines of one record type (``"@SQ"``, ``"@PG"`` ...)."""
+        prefix = kind + "\t"
+        return [ln for ln in self.text.split("\n") if ln.startswith(prefix)]
 
 
 def _strings_at(data: torch.Tensor, offset: torch.Tensor, length: torch.Tensor) -> StringColumn:

@@ -5,7 +5,9 @@ Same API and chunk semantics as cubam's ``src/cubam/bgzf.py`` read side
 ``:542-612``, ``_ChunkReader`` ``:38-125``), on this package's kernels:
 
 1. **Read.** A background thread reads the next chunks into pinned host
-   buffers with parallel ``pread`` calls (``_ChunkReader``).
+   slots with parallel ``preadv`` calls and copies each to the device on a
+   stream of its own; the consumer waits on the copy's event
+   (``_ChunkReader``).
 2. **Find members.** ``cb_scan_members``: 128-bit loads and byte matching find
    every BGZF header, the chain from offset 0 is kept and checked, and one
    inflate job per non-empty member is written with its output offset.  The
@@ -20,7 +22,6 @@ cubam does not check) is a ``ValueError`` too, unless ``check_crc=False``.
 from __future__ import annotations
 
 import os
-import queue
 import threading
 from collections.abc import Iterator
 from pathlib import Path
@@ -77,84 +78,121 @@ def read_struct(t: torch.Tensor, cls):
 
 
 class _ChunkReader:
-    """Chunks of a file read ahead into pinned buffers by a background thread.
+    """The chunks of a file on the device, read ahead by one background thread.
 
-    Each chunk is read by ``n_threads`` parallel ``pread`` calls of ``piece``
-    bytes.  Iterating yields ``(slot, nbytes, eof)``; the consumer copies
-    :meth:`host` ``(slot)[:nbytes]`` to the GPU and then calls :meth:`release`.
+    The thread fills pinned host slots (``n_buffers`` of ``chunk_bytes``) in turn: a chunk is read
+    by ``n_threads`` workers with ``os.preadv`` of ``piece`` bytes each, straight into its slot,
+    then the thread issues the slot's copy to a fresh device buffer on a CUDA stream of its own and
+    records an event.  Iterating yields ``(chunk, eof)``: the consumer's current stream waits on
+    the copy's event (no host wait), so the copies of the chunks ahead run under the kernels of
+    the current one.  A slot is refilled once the copy out of it has completed, and at most
+    ``n_buffers`` chunks are read ahead of the consumer.
+
+    An exception in the thread (an unreadable file, a short read) reaches the consumer at the first
+    chunk it has not delivered.  Without CUDA the chunks are host tensors (no pinned memory, no
+    stream), which is how the reading logic is tested on a host without a GPU.
     """
 
     def __init__(self, path, chunk_bytes: int, *, n_buffers: int = 3, n_threads: int = 8, piece: int = 16 << 20):
-        self.path, self.chunk, self.n_threads, self.piece = Path(path), chunk_bytes, n_threads, max(int(piece), 1)
-        pin = torch.cuda.is_available()  # page-locked for the H2D copies; plain memory on a host without CUDA
-        self._mem = [torch.empty(chunk_bytes, dtype=torch.uint8, pin_memory=pin) for _ in range(n_buffers)]
-        self._free: queue.Queue = queue.Queue()
-        for i in range(n_buffers):
-            self._free.put(i)
-        self._full: queue.Queue = queue.Queue()
-        self._error: BaseException | None = None
-        self._stop = False
-        self._thread = threading.Thread(target=self._run, daemon=True)
+        self.path, self.chunk = Path(path), int(chunk_bytes)
+        self.n_buffers, self.n_threads, self.piece = max(int(n_buffers), 1), max(int(n_threads), 1), max(int(piece), 1)
+        self._cuda = torch.cuda.is_available()
+        self._device = torch.cuda.current_device() if self._cuda else None
+        self._slots = [torch.empty(self.chunk, dtype=torch.uint8, pin_memory=self._cuda) for _ in range(self.n_buffers)]
+        self._cv = threading.Condition()
+        self._ready: dict[int, tuple] = {}  # chunk index -> (tensor, eof, event)
+        self._delivered = 0                  # chunks handed to the consumer
+        self._failure: BaseException | None = None
+        self._closed = False
+        self._thread = threading.Thread(target=self._produce, name="cubam-reader", daemon=True)
         self._thread.start()
 
-    def host(self, slot: int) -> torch.Tensor:
-        return self._mem[slot]
-
-    def release(self, slot: int) -> None:
-        self._free.put(slot)
-
     def close(self) -> None:
-        self._stop = True
-        self._free.put(-1)
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
 
     @staticmethod
-    def _pread(fd: int, mv: memoryview, offset: int) -> None:
-        while len(mv):
-            got = os.preadv(fd, [mv], offset)
-            if not got:
+    def _read_piece(fd: int, dst: memoryview, offset: int) -> None:
+        """Fill ``dst`` from ``offset`` of the file (pread until it is full)."""
+        while len(dst):
+            got = os.preadv(fd, [dst], offset)
+            if got <= 0:
                 raise ValueError("The file is shorter than its size")
-            mv, offset = mv[got:], offset + got
+            dst, offset = dst[got:], offset + got
 
-    def _run(self) -> None:
+    def _produce(self) -> None:
         from concurrent.futures import ThreadPoolExecutor
 
         try:
+            if self._cuda:
+                torch.cuda.set_device(self._device)
+                stream = torch.cuda.Stream()
+            copied: list = [None] * self.n_buffers  # event of the last copy out of each slot
             fd = os.open(self.path, os.O_RDONLY)
             try:
                 size = os.fstat(fd).st_size
-                off = 0
-                with ThreadPoolExecutor(self.n_threads) as ex:
+                with ThreadPoolExecutor(self.n_threads) as workers:
+                    k = off = 0
                     while True:
-                        slot = self._free.get()
-                        if self._stop:
-                            return
+                        with self._cv:
+                            while not self._closed and k - self._delivered >= self.n_buffers:
+                                self._cv.wait()
+                            if self._closed:
+                                return
+                        slot = k % self.n_buffers
+                        if copied[slot] is not None:
+                            copied[slot].synchronize()  # the slot's previous chunk has left it
                         n = min(self.chunk, size - off)
-                        mv = memoryview(self._mem[slot].numpy())
-                        futures = [
-                            ex.submit(self._pread, fd, mv[p : min(p + self.piece, n)], off + p)
-                            for p in range(0, n, self.piece)
-                        ]
-                        for f in futures:
-                            f.result()
+                        view = memoryview(self._slots[slot].numpy())[:n]
+                        reads = [workers.submit(self._read_piece, fd, view[p : p + self.piece], off + p)
+                                 for p in range(0, n, self.piece)]
+                        for r in reads:
+                            r.result()
+                        ev = None
+                        if self._cuda:
+                            with torch.cuda.stream(stream):
+                                chunk = torch.empty(n, dtype=torch.uint8, device=self._device)
+                                chunk.copy_(self._slots[slot][:n], non_blocking=True)
+                                ev = torch.cuda.Event()
+                                ev.record(stream)
+                            copied[slot] = ev
+                        else:
+                            chunk = self._slots[slot][:n].clone()
                         off += n
                         eof = off >= size
-                        self._full.put((slot, n, eof))
+                        with self._cv:
+                            self._ready[k] = (chunk, eof, ev)
+                            self._cv.notify_all()
                         if eof:
                             return
+                        k += 1
             finally:
                 os.close(fd)
-        except BaseException as e:  # noqa: BLE001  (re-raised in the consumer)
-            self._error = e
-            self._full.put(None)
+        except BaseException as e:  # noqa: BLE001  (raised in the consumer)
+            with self._cv:
+                self._failure = e
+                self._cv.notify_all()
 
-    def __iter__(self) -> Iterator[tuple[int, int, bool]]:
+    def __iter__(self) -> Iterator[tuple[torch.Tensor, bool]]:
+        k = 0
         while True:
-            item = self._full.get()
-            if item is None:
-                raise self._error  # type: ignore[misc]
-            yield item
-            if item[2]:
+            with self._cv:
+                while k not in self._ready and self._failure is None:
+                    self._cv.wait()
+                if k not in self._ready:
+                    raise self._failure  # type: ignore[misc]
+                chunk, eof, ev = self._ready.pop(k)
+                self._delivered = k + 1
+                self._cv.notify_all()
+            if ev is not None:
+                cur = torch.cuda.current_stream()
+                cur.wait_event(ev)
+                chunk.record_stream(cur)  # allocated on the reader's stream, used on this one
+            yield chunk, eof
+            if eof:
                 return
+            k += 1
 
 
 def _workspace(nbytes: int) -> torch.Tensor:
@@ -253,33 +291,11 @@ def _inflate(path: str | Path, chunk_bytes: int | None, prefix, check_crc: bool 
 
     chunk_bytes = chunk_bytes or auto_chunk_bytes()
     reader = _ChunkReader(path, chunk_bytes, **reader_kw)
-    carry = torch.empty(0, dtype=torch.uint8, device="cuda")
-    copies = torch.cuda.Stream()  # host-to-device copies of the next chunk overlap the work on this one
-
-    def upload(item):
-        slot, nbytes, eof = item
-        dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
-        copies.wait_stream(torch.cuda.current_stream())  # dev's memory may have been in use there
-        with torch.cuda.stream(copies):
-            dev.copy_(reader.host(slot)[:nbytes], non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record(copies)
-        return slot, eof, dev, ev
-
+    carry = torch.empty(0, dtype=torch.uint8, device="cuda")  # the incomplete last member, compressed
     try:
-        chunks = iter(reader)
-        first = next(chunks, None)
-        cur = upload(first) if first is not None else None
-        while cur is not None:
-            slot, eof, dev, ev = cur
-            ev.synchronize()
-            reader.release(slot)  # the host slot is copied: the reader may fill it again
-            nxt = next(chunks, None)
-            cur = upload(nxt) if nxt is not None else None
-            torch.cuda.current_stream().wait_event(ev)
-            c = int(carry.numel())
-            buf = torch.cat([carry, dev]) if c else dev
-            del dev
+        for chunk, eof in reader:
+            buf = torch.cat([carry, chunk]) if carry.numel() else chunk
+            del chunk
             res = _inflate_blocks(buf, eof, prefix and prefix(), check_crc, defer_check)
             data, used = res[0], res[1]
             carry = buf[used:].clone()

@@ -176,95 +176,146 @@ def _bgzf_compress(data, level: int = 2, block_off=None, block_size=None, return
 
 
 class BgzfWriter:
-    """A BGZF file written from data on the GPU (``src/cubam/bgzf.py:425-539``).
+    """A BGZF file written from data on the GPU (the API of cubam's ``BgzfWriter``,
+    ``src/cubam/bgzf.py:425-539``: ``write``, ``flush``, ``close``, a context manager; the same
+    blocks for the same calls).
 
-    :meth:`write` appends bytes (a device uint8 tensor, or bytes); full blocks are compressed on
-    the GPU once ``flush_bytes`` are buffered.  :meth:`close` compresses the rest and adds the EOF
-    block.  The compressed blocks are copied to one of two pinned host buffers and written by
-    background threads (parallel ``pwrite`` of ``piece``-byte pieces) while the GPU goes on.
+    Bytes given to :meth:`write` (a device uint8 tensor, or bytes) are appended to one staging
+    buffer on the device.  Once ``flush_bytes`` are staged, every whole ``BLOCK_DATA`` block of them
+    is compressed (:func:`_bgzf_compress`) and the remainder moves to the front of the buffer;
+    :meth:`flush` and :meth:`close` compress everything staged.  Each compressed batch is copied to
+    a pinned host buffer on a CUDA stream of its own, and a writer thread waits for that copy's event
+    and writes the batch at its offset in the file (``n_threads`` parallel ``pwrite`` of ``piece``
+    bytes), so compression and disk writes overlap; two batches at most are in flight.  A failed
+    write is raised by the next call.  :meth:`close` writes the EOF block after the last batch.
     """
+
+    _IN_FLIGHT = 2
 
     def __init__(self, path: str | Path, level: int = 2, flush_bytes: int = 1024 * BLOCK_DATA, *, n_threads: int = 8,
                  piece: int = 16 << 20):
+        import queue
+        import threading
         from concurrent.futures import ThreadPoolExecutor
 
         self.path = Path(path)
         self.level = level
-        self.flush_bytes = flush_bytes
-        self._fh = open(self.path, "wb")  # noqa: SIM115  (closed in close())
-        self._pending: list[torch.Tensor] = []
-        self._n = 0
-        self._io = ThreadPoolExecutor(n_threads)
-        self._piece = piece
-        self._pos = 0
-        self._host: list = [None, None]
-        self._writes: list = [[], []]
-        self._turn = 0
+        self.flush_bytes = int(flush_bytes)
+        self._fd = os.open(self.path, os.O_WRONLY | os.O_CREAT | os.O_TRUNC, 0o666)
+        self._open = True
+        self._stage = torch.empty(max(self.flush_bytes + BLOCK_DATA, BLOCK_DATA), dtype=torch.uint8, device="cuda")
+        self._staged = 0
+        self._end = 0  # file offset after the batches handed to the writer thread
+        self._piece = max(int(piece), 1)
+        self._copy_stream = torch.cuda.Stream()
+        self._room = threading.Semaphore(self._IN_FLIGHT)
+        self._spare: list[torch.Tensor] = []  # pinned buffers back from the writer thread
+        self._batches: queue.SimpleQueue = queue.SimpleQueue()
+        self._failure: BaseException | None = None
+        self._pool = ThreadPoolExecutor(max(int(n_threads), 1))
+        self._writer = threading.Thread(target=self._write_batches, name="cubam-bgzf-writer", daemon=True)
+        self._writer.start()
 
-    @staticmethod
-    def _pwrite(fd: int, mv: memoryview, offset: int) -> None:
+    # ---------------------------------------------------------------- the writer thread
+    def _pwrite_all(self, mv: memoryview, offset: int) -> None:
         while len(mv):
-            n = os.pwrite(fd, mv, offset)
-            mv, offset = mv[n:], offset + n
+            k = os.pwrite(self._fd, mv, offset)
+            mv, offset = mv[k:], offset + k
 
-    def _put(self, out: torch.Tensor) -> None:
-        """Copy ``out`` to a pinned buffer and write it in the background."""
-        i, self._turn = self._turn, self._turn ^ 1
-        for f in self._writes[i]:
-            f.result()  # the buffer is free again
-        n = int(out.numel())
-        if self._host[i] is None or self._host[i].numel() < n:
-            self._host[i] = torch.empty(max(n, 2 * self.flush_bytes), dtype=torch.uint8, pin_memory=True)
-        host = self._host[i][:n]
-        host.copy_(out)
-        mv, fd = memoryview(host.numpy()), self._fh.fileno()
-        self._writes[i] = [
-            self._io.submit(self._pwrite, fd, mv[a : a + self._piece], self._pos + a) for a in range(0, n, self._piece)
-        ]
-        self._pos += n
+    def _write_batches(self) -> None:
+        while True:
+            item = self._batches.get()
+            if item is None:
+                return
+            host, n, offset, done = item
+            try:
+                if self._failure is None:
+                    if done is not None:
+                        done.synchronize()  # the device-to-host copy of this batch
+                    mv = memoryview(host.numpy())[:n]
+                    parts = [self._pool.submit(self._pwrite_all, mv[a : a + self._piece], offset + a)
+                             for a in range(0, n, self._piece)]
+                    for f in parts:
+                        f.result()
+            except BaseException as e:  # noqa: BLE001  (raised by the next call of the owner)
+                self._failure = e
+            finally:
+                self._spare.append(host)
+                self._room.release()
 
-    def _drain(self) -> None:
-        for i, fs in enumerate(self._writes):
-            self._writes[i] = []
-            for f in fs:
-                f.result()
+    # ---------------------------------------------------------------- the caller's side
+    def _raise_failure(self) -> None:
+        if self._failure is not None:
+            raise self._failure
+
+    def _emit(self, blocks: torch.Tensor) -> None:
+        """Hand one batch of BGZF blocks (device) to the writer thread, at the next file offset."""
+        n = int(blocks.numel())
+        if n == 0:
+            return
+        self._room.acquire()
+        if self._failure is not None:
+            self._room.release()
+            raise self._failure
+        host = next((b for b in self._spare if b.numel() >= n), None)
+        if host is not None:
+            self._spare.remove(host)
+        else:
+            host = torch.empty(max(n, 2 * self.flush_bytes), dtype=torch.uint8, pin_memory=True)
+        cs = self._copy_stream
+        cs.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(cs):
+            host[:n].copy_(blocks, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(cs)
+        blocks.record_stream(cs)
+        self._batches.put((host, n, self._end, done))
+        self._end += n
+
+    def _compress_staged(self, everything: bool) -> None:
+        cut = self._staged if everything else self._staged // BLOCK_DATA * BLOCK_DATA
+        if cut:
+            self._emit(_bgzf_compress(self._stage[:cut], self.level))
+            rest = self._staged - cut
+            if rest:  # less than one block: moved to the front
+                self._stage[:rest].copy_(self._stage[cut : cut + rest].clone())
+            self._staged = rest
 
     def write(self, data) -> None:
+        self._raise_failure()
         data = _as_bytes(data)
-        if data.numel():
-            self._pending.append(data)
-            self._n += int(data.numel())
-        if self._n >= self.flush_bytes:
-            self._flush(final=False)
-
-    def _flush(self, final: bool) -> None:
-        if not self._pending:
-            return
-        buf = torch.cat(self._pending) if len(self._pending) > 1 else self._pending[0]
-        cut = int(buf.numel()) if final else int(buf.numel()) // BLOCK_DATA * BLOCK_DATA
-        if cut:
-            self._put(_bgzf_compress(buf[:cut], self.level))
-        rest = buf[cut:]
-        self._pending = [rest.clone()] if rest.numel() else []
-        self._n = int(rest.numel())
+        n = int(data.numel())
+        if n:
+            need = self._staged + n
+            if need > self._stage.numel():
+                grown = torch.empty(max(need, 2 * self._stage.numel()), dtype=torch.uint8, device="cuda")
+                grown[: self._staged].copy_(self._stage[: self._staged])
+                self._stage = grown
+            self._stage[self._staged : need].copy_(data)
+            self._staged = need
+        if self._staged >= self.flush_bytes:
+            self._compress_staged(everything=False)
 
     def flush(self) -> None:
         """Compress and write what is buffered, so that the next bytes start a new block."""
-        self._flush(final=True)
+        self._compress_staged(everything=True)
 
     def close(self) -> None:
-        if self._fh.closed:
+        if not self._open:
             return
+        self._open = False
         try:
-            self._flush(final=True)
-            self._drain()
-            self._pwrite(self._fh.fileno(), memoryview(EOF_BLOCK), self._pos)
+            self._compress_staged(everything=True)
+            self._room.acquire()
+            eof = torch.frombuffer(bytearray(EOF_BLOCK), dtype=torch.uint8)
+            self._batches.put((eof, len(EOF_BLOCK), self._end, None))
+            self._end += len(EOF_BLOCK)
         finally:
-            try:
-                self._drain()
-            finally:
-                self._io.shutdown()
-                self._fh.close()
+            self._batches.put(None)
+            self._writer.join()
+            self._pool.shutdown()
+            os.close(self._fd)
+        self._raise_failure()
 
     def __enter__(self) -> BgzfWriter:
         return self

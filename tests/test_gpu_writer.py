@@ -211,3 +211,40 @@ def test_streams_equal_the_host_model_byte_for_byte(tmp_path, host_model, level)
     assert len(want) == len(off)
     for i, (a, b) in enumerate(zip(oo, osz, strict=True)):
         assert got[a : a + b] == want[i], (i, off[i], size[i])
+
+
+def test_writer_flush_ends_blocks_and_failures_are_raised(tmp_path, monkeypatch):
+    """flush() ends a block early (the oracle's block sizes); a write that fails in the writer thread is
+    raised by the owner's next call."""
+    import os
+
+    from cubam_b200.bgzf import EOF_BLOCK, BgzfWriter
+
+    rng = np.random.default_rng(5)
+    parts = [rng.integers(65, 70, k, dtype=np.uint8).tobytes() for k in (1000, 70_000, 5, 200_000, 65_280)]
+    p = tmp_path / "f.gz"
+    with BgzfWriter(p, flush_bytes=100_000) as w:
+        for i, part in enumerate(parts):
+            w.write(dev(part))
+            if i in (0, 2):
+                w.flush()
+    assert gzip.decompress(p.read_bytes()) == b"".join(parts)
+    sizes = [m["isize"] for m in W.members(p.read_bytes()[: -len(EOF_BLOCK)])]
+    assert sizes == W.writer_blocks(parts, 100_000, flushes=(0, 2))
+    real = os.pwrite
+    calls = []
+
+    def failing(fd, data, offset):
+        calls.append(offset)
+        if len(calls) > 1:
+            raise OSError(28, "injected: no space left")
+        return real(fd, data, offset)
+
+    monkeypatch.setattr(os, "pwrite", failing)
+    w = BgzfWriter(tmp_path / "g.gz", flush_bytes=65_280, n_threads=1)
+    with pytest.raises(OSError, match="injected"):
+        try:
+            for part in parts * 3:
+                w.write(dev(part))
+        finally:
+            w.close()

@@ -40,13 +40,23 @@ def test_chunk_reader_reads_the_file_in_slots(tmp_path):
     from cubam_b200.bgzf import _ChunkReader
 
     raw = (GOLDEN / "text_b1000.gz").read_bytes()
-    r = _ChunkReader(GOLDEN / "text_b1000.gz", 10_000, n_buffers=2, n_threads=3, piece=3333)
-    got = bytearray()
-    for slot, n, eof in r:
-        got += r.host(slot)[:n].numpy().tobytes()
-        r.release(slot)
-    r.close()
-    assert bytes(got) == raw
+    for n_buffers in (1, 2, 3):
+        r = _ChunkReader(GOLDEN / "text_b1000.gz", 10_000, n_buffers=n_buffers, n_threads=3, piece=3333)
+        got, flags = bytearray(), []
+        for chunk, eof in r:
+            got += chunk.cpu().numpy().tobytes()
+            flags.append(eof)
+        r.close()
+        assert bytes(got) == raw
+        assert flags[-1] and not any(flags[:-1])
+
+
+def test_chunk_reader_empty_file(tmp_path):
+    from cubam_b200.bgzf import _ChunkReader
+
+    p = tmp_path / "empty"
+    p.write_bytes(b"")
+    assert [(int(c.numel()), eof) for c, eof in _ChunkReader(p, 4096)] == [(0, True)]
 
 
 def test_chunk_reader_error_reaches_the_consumer(tmp_path):
@@ -57,3 +67,80 @@ def test_chunk_reader_error_reaches_the_consumer(tmp_path):
     r = _ChunkReader(tmp_path / "missing.bam", 4096)
     with pytest.raises(FileNotFoundError):
         list(r)
+
+
+def test_chunk_reader_fault_in_the_thread_reaches_the_consumer(tmp_path, monkeypatch):
+    """A read that fails in the reader thread after some chunks (injected on the host): the consumer
+    gets every chunk read before it, then the exception itself."""
+    import pytest
+
+    from cubam_b200.bgzf import _ChunkReader
+
+    p = tmp_path / "data"
+    p.write_bytes(bytes(range(256)) * 100)  # 25,600 bytes: chunks of 4096
+    real = _ChunkReader._read_piece
+
+    def flaky(fd, dst, offset):
+        if offset >= 3 * 4096:
+            raise OSError(5, "injected read failure")
+        real(fd, dst, offset)
+
+    monkeypatch.setattr(_ChunkReader, "_read_piece", staticmethod(flaky))
+    got = []
+    with pytest.raises(OSError, match="injected read failure"):
+        for chunk, _ in _ChunkReader(p, 4096, n_buffers=2, n_threads=2, piece=1000):
+            got.append(chunk.cpu().numpy().tobytes())
+    assert b"".join(got) == p.read_bytes()[: 3 * 4096]
+
+
+def test_chunk_reader_short_file_message(tmp_path, monkeypatch):
+    """The file shrinking under the reader gives the reference's message."""
+    import os
+
+    import pytest
+
+    from cubam_b200.bgzf import _ChunkReader
+
+    p = tmp_path / "data"
+    p.write_bytes(b"x" * 10_000)
+    monkeypatch.setattr(os, "fstat", lambda fd: os.stat_result((0, 0, 0, 0, 0, 0, 20_000, 0, 0, 0)))
+    with pytest.raises(ValueError, match="The file is shorter than its size"):
+        list(_ChunkReader(p, 4096))
+
+
+def test_header_errors_and_round_trip(tmp_path):
+    import gzip
+    import struct
+
+    import pytest
+
+    from cubam_b200 import BamHeader
+    from cubam_b200.bgzf import EOF_BLOCK
+
+    h = BamHeader.read(GOLDEN / "mixed_b700.bam")
+    # the header bytes written back as gzip members of one byte each: the header spans many members
+    blob = h.to_bytes()
+    members = b"".join(gzip.compress(blob[i : i + 1]) for i in range(len(blob)))
+    p = tmp_path / "split.bam"
+    p.write_bytes(members + EOF_BLOCK)
+    h2 = BamHeader.read(p)
+    assert h2 == h and h2.size == len(blob)
+    t = h.to_bytes("@HD\tVN:1.6\tSO:queryname\n@PG\tID:x\n")
+    p.write_bytes(gzip.compress(t))
+    h3 = BamHeader.read(p)
+    assert h3.sort_order == "queryname" and h3.lines("@PG") == ["@PG\tID:x"]
+    with pytest.raises(ValueError, match="not coordinate-sorted"):
+        h3.require_coordinate_sorted(p)
+    p.write_bytes(gzip.compress(b"BAM\2" + blob[4:]))
+    with pytest.raises(ValueError, match="not a BAM file"):
+        BamHeader.read(p)
+    p.write_bytes(gzip.compress(blob[:-3]))
+    with pytest.raises(ValueError, match="truncated BAM header"):
+        BamHeader.read(p)
+    p.write_bytes(gzip.compress(b"BAM\1" + struct.pack("<i", -5)))
+    with pytest.raises(ValueError, match="truncated BAM header"):
+        BamHeader.read(p)
+    p.write_bytes(b"plain text, not gzip")
+    with pytest.raises(gzip.BadGzipFile):
+        BamHeader.read(p)
+    assert BamHeader("", [], [], 0).sort_order == "unknown"
