@@ -17,6 +17,8 @@ LIB_PATH = _build.LIB
 
 # status codes (include/cubam_b200.h)
 OK, TRUNCATED, NO_CHAIN, CORRUPT_BLOCK, INFLATE, CRC, TOO_MANY, CAPACITY, CUDA, ARG, TIMEOUT = range(11)
+#: launch parameters (cb_set_param / cb_get_param)
+PARAM_CHAIN_TILE, PARAM_INFLATE_FORM, PARAM_DECODE_ROOT, PARAM_COPY_WARPS, PARAM_DECODE_STEPS = range(1, 6)
 
 
 class MemberJob(ctypes.Structure):
@@ -69,6 +71,8 @@ _SIGNATURES = {
     "cb_version": (c_char_p, []),
     "cb_last_error": (c_char_p, []),
     "cb_device_sm_count": (c_int, []),
+    "cb_set_param": (c_int, [c_int, I64]),
+    "cb_get_param": (I64, [c_int]),
     "cb_scan_workspace_bytes": (c_size_t, [I64]),
     "cb_scan_members": (c_int, [P, I64, c_int, I64, P, I64, P, P, c_size_t, P]),
     "cb_scan_members_noalloc": (c_int, [P, I64, c_int, I64, P, I64, P, P]),
@@ -76,6 +80,8 @@ _SIGNATURES = {
     "cb_inflate": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, P]),
     "cb_inflate_form": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, c_int, P]),
     "cb_inflate_lane_slots": (I64, []),
+    "cb_inflate_split_workspace_bytes": (c_size_t, [I64, I64]),
+    "cb_inflate_split": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, P]),
     "cb_record_chain_workspace_bytes": (c_size_t, [I64]),
     "cb_record_chain": (c_int, [P, I64, c_int32, P, I64, P, P, c_size_t, P]),
     "cb_decode_fixed": (c_int, [P, P, I64] + [P] * 11 + [P]),

@@ -223,10 +223,20 @@ def inflate_jobs(jobs: torch.Tensor, n_jobs: int, out: torch.Tensor, check_crc: 
                  job_status: torch.Tensor | None = None) -> torch.Tensor:
     """Launch ``cb_inflate_form`` of ``n_jobs`` jobs into ``out``; returns the device summary (no sync).
 
-    ``form`` 0 lets the library choose (as ``cb_inflate``), 1 is one member per warp, 2 one per lane.
+    ``form`` 0 lets the library choose (as ``cb_inflate``), 1 is one member per warp, 2 one per lane,
+    3 the two-kernel form (``cb_inflate_split``: decode one member per lane, copy one per warp).
     ``job_status`` (device uint32/int32 of ``n_jobs``) receives a status code per job when given.
     """
     summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device="cuda")
+    if form == 3:
+        ws = _workspace(_lib.lib.cb_inflate_split_workspace_bytes(n_jobs, int(out.numel())))
+        rc = _lib.lib.cb_inflate_split(
+            jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc),
+            job_status.data_ptr() if job_status is not None else None,
+            summ.data_ptr(), ws.data_ptr(), ws.numel(), stream_ptr(),
+        )
+        _lib.check(rc, "cb_inflate_split")
+        return summ
     ws = _workspace(_lib.lib.cb_inflate_workspace_bytes())
     rc = _lib.lib.cb_inflate_form(
         jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc),

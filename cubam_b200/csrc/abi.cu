@@ -1,5 +1,6 @@
 // Library-wide entry points of the C ABI: version, error text, device properties.
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -21,6 +22,56 @@ int cb_set_error_text(int code, const char* text) {
 extern "C" const char* cb_version(void) { return "cubam_b200 0.1.0 (sm_100a)"; }
 
 extern "C" const char* cb_last_error(void) { return g_err; }
+
+// ---- launch parameters: one value per key for the process, read at every launch
+namespace {
+struct Param {
+    int key;
+    int64_t lo, hi, def;
+};
+constexpr Param kParams[] = {
+    {CB_PARAM_CHAIN_TILE, 2048, 1 << 22, 32768},
+    {CB_PARAM_INFLATE_FORM, 1, 3, 1},
+    {CB_PARAM_DECODE_ROOT, 8, 9, 8},
+    {CB_PARAM_COPY_WARPS, 1, 6, 3},
+    {CB_PARAM_DECODE_STEPS, 1, 64, 16},
+};
+constexpr int kNParams = sizeof(kParams) / sizeof(kParams[0]);
+std::atomic<int64_t> g_param[kNParams] = {};
+std::atomic<bool> g_param_set[kNParams] = {};
+
+int param_index(int key) {
+    for (int i = 0; i < kNParams; i++)
+        if (kParams[i].key == key) return i;
+    return -1;
+}
+}  // namespace
+
+int64_t cb_param(int key) {
+    const int i = param_index(key);
+    if (i < 0) return 0;
+    return g_param_set[i].load(std::memory_order_acquire) ? g_param[i].load(std::memory_order_relaxed) : kParams[i].def;
+}
+
+extern "C" int64_t cb_get_param(int key) { return param_index(key) < 0 ? -1 : cb_param(key); }
+
+extern "C" int cb_set_param(int key, int64_t value) {
+    const int i = param_index(key);
+    if (i < 0) return cb_set_error_text(CB_ERR_ARG, "cb_set_param: unknown key");
+    if (value == 0) {  // back to the default
+        g_param_set[i].store(false, std::memory_order_release);
+        return CB_OK;
+    }
+    if (value < kParams[i].lo || value > kParams[i].hi)
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
+    if (key == CB_PARAM_CHAIN_TILE && (value & (value - 1)))
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is a power of two");
+    if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6)
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3 or 6");
+    g_param[i].store(value, std::memory_order_relaxed);
+    g_param_set[i].store(true, std::memory_order_release);
+    return CB_OK;
+}
 
 extern "C" int cb_device_sm_count(void) {
     static int cache[64] = {0};

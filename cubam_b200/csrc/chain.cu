@@ -6,7 +6,7 @@
 // follows block_size while the predicate holds, which is O(records), not O(bytes).  It is walked in
 // parallel by tiles:
 //
-//  1. k_walk: one thread per 2 KB tile finds the tile's first offset that passes the predicate and
+//  1. k_walk: one thread per tile (CB_PARAM_CHAIN_TILE bytes, 32 KB unless tuned) finds the tile's first offset that passes the predicate and
 //     walks the block_size links from it (each record checked with the full predicate) up to the first
 //     offset past the tile: first[t], count[t], exit[t], and whether the walk broke inside the tile.
 //  2. k_check: tile t's walk is the true chain when its first offset is where the previous non-empty
@@ -22,9 +22,9 @@
 namespace cb {
 namespace chain {
 
-constexpr long long T = 2048;   // bytes per tile
+constexpr long long T_MIN = 2048;  // smallest tile (the workspace is sized for it)
 constexpr int NT = 256;
-constexpr int SCAN = 1024;       // tiles per block of the count scan
+constexpr int SCAN = 1024;         // tiles per block of the count scan
 
 struct Ws {
     int64_t* first;    // per tile
@@ -34,12 +34,14 @@ struct Ws {
     int64_t* bsum;     // per scan block
     int64_t* meta;     // [0] inconsistent tile (min) [1] first broken tile (min) [2] any candidate [3] total
     long long ntiles, nblocks;
+    long long T;       // bytes per tile
 };
 
 __host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-__host__ __device__ inline Ws carve(void* ws, long long n) {
+__host__ __device__ inline Ws carve(void* ws, long long n, long long T) {
     Ws w;
+    w.T = T;
     w.ntiles = (n + T - 1) / T;
     if (w.ntiles < 1) w.ntiles = 1;
     w.nblocks = (w.ntiles + SCAN - 1) / SCAN;
@@ -59,7 +61,7 @@ __host__ __device__ inline Ws carve(void* ws, long long n) {
 }
 
 __host__ inline size_t ws_bytes(long long n) {
-    long long ntiles = (n + T - 1) / T;
+    long long ntiles = (n + T_MIN - 1) / T_MIN;
     if (ntiles < 1) ntiles = 1;
     long long nblocks = (ntiles + SCAN - 1) / SCAN;
     return 256 + 3 * align256(ntiles * 8) + align256(ntiles * 4) + align256(nblocks * 8) + 256;
@@ -128,7 +130,7 @@ __global__ void k_init(Ws w) {
 __global__ void __launch_bounds__(NT) k_walk(const uint8_t* b, long long n, int n_ref, Ws w) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
          t += (long long)gridDim.x * blockDim.x) {
-        const long long ts = t * T, te = min(ts + T, n);
+        const long long ts = t * w.T, te = min(ts + w.T, n);
         const long long c = first_candidate(b, n, ts, te, n_ref);
         long long o = c;
         int cnt = 0;
@@ -279,7 +281,7 @@ extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, in
     if (n < 0 || !summary || !workspace || (n > 0 && (!data || !offsets)) || cap < 0) return CB_ERR_ARG;
     if (workspace_bytes < chain::ws_bytes(n)) return CB_ERR_CAPACITY;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    chain::Ws w = chain::carve(workspace, n);
+    chain::Ws w = chain::carve(workspace, n, cb_param(CB_PARAM_CHAIN_TILE));
     const long long sms = cb_device_sm_count();
     long long grid = (w.ntiles + chain::NT - 1) / chain::NT;
     if (grid > sms * 16) grid = sms * 16;

@@ -6,6 +6,9 @@
 
 #include "../../include/cubam_b200.h"
 
+// The current value of a launch parameter (abi.cu; cb_set_param / cb_get_param).
+int64_t cb_param(int key);
+
 namespace cb {
 
 constexpr unsigned FULL = 0xffffffffu;

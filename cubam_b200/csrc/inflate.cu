@@ -1414,7 +1414,14 @@ extern "C" int cb_inflate_form(const cb_member_job* jobs, int64_t n_jobs, const 
                                int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
                                size_t workspace_bytes, int form, void* stream) {
     if (!summary || !workspace || workspace_bytes < cb_inflate_workspace_bytes() || n_jobs < 0) return CB_ERR_ARG;
-    if (form == 0) form = 1;  // measured ahead of form 2 from 7.7 k to 193 k members (GEX, B200)
+    if (form == 0) form = (int)cb_param(CB_PARAM_INFLATE_FORM);
+    if (form == 3) {
+        // the split form needs its token arena: a workspace of the forms-1/2 size runs form 1 instead
+        if (workspace_bytes > cb_inflate_workspace_bytes())
+            return cb_inflate_split(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, workspace,
+                                    workspace_bytes, stream);
+        form = 1;
+    }
     if (form != 1 && form != 2) return CB_ERR_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     auto* queue = reinterpret_cast<unsigned long long*>(workspace);

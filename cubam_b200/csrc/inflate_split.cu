@@ -1,0 +1,841 @@
+// Raw-DEFLATE inflater for BGZF members, form 3: the Huffman decode and the copy in two kernels.
+//
+// Replaces cubam's nvcompBatchedDeflateDecompressAsync call and its status/size check
+// (src/cubam/bgzf.py:587-611) with the CRC32 check added (cubam's reader does not check it,
+// docs/reading.md:48-51).  DEFLATE is RFC 1951.
+//
+// Why two kernels.  Huffman decoding is serial within a member, and the copy of a back-reference
+// needs the member's output up to 32 KiB back.  In BGZF files of BAM records most references reach
+// far (on the GEX-shaped workload the median distance is about 3 KB and only 7% are within 224
+// bytes), so a decoder that also copies either keeps 32 KiB per member on chip (few members in
+// flight, idle issue slots) or reads HBM at every match (long waits).  Here:
+//
+//  1. k_decode: one member per LANE.  32 members per warp advance one symbol per step in lock step,
+//     each lane with its own tables in shared memory (16-bit entries, 2^LB literal/length and 2^DB
+//     distance root entries; longer codes by per-length limits kept in registers), and write the
+//     symbols as 16-bit units to a token arena in HBM: a literal is one unit, a match two (length and
+//     the high distance bits, then the low distance bits).  Block headers, code lengths and stored
+//     blocks are steps of the same lock-step loop; the code tables of one lane are built by the
+//     whole warp.  The output size, distances and the end of the payload are checked here.
+//  2. k_copy: one member per WARP.  The warp reads its member's units 32 at a time, places them by
+//     a prefix sum of their lengths, and writes the bytes 32 at a time into a 32 KiB ring in shared
+//     memory (every DEFLATE distance reads the ring); a byte whose source lies in the same 32 bytes
+//     takes it from another lane.  Completed 1 KiB windows go to HBM with 16-byte stores and into
+//     the CRC32 (32 lane columns joined in GF(2)).
+//
+// Units are at most one per output byte, so a member's units take at most 2 ISIZE bytes: the arena
+// holds member i at an 8-byte aligned slot from 2 out_off + 16 i (jobs in increasing out_off with
+// disjoint outputs, as the member scan writes them; a job out of that order is a CB_ERR_ARG of its
+// own).
+//
+// Every loop is bounded: each decode step consumes input bits or produces output bytes, both
+// bounded per member; every shared-memory index is masked or checked; arena and output writes
+// stay within the member's slot and output range.
+
+#include "common.cuh"
+#include "crc.cuh"
+
+namespace cb {
+namespace split {
+
+// ---------------------------------------------------------------- formats
+
+// 16-bit table entries (k_decode).
+//   bit 15 set: a length symbol: bits 12-14 extra bits, 8-11 code length, 0-7 base - 3.
+//   bit 15 clear: bits 12-14 kind, 8-11 code length, 0-7 value:
+//     0 literal (value: the byte), 1 end of block, 2 distance (value: symbol 0-29),
+//     3 special (value 0: a code longer than the root bits; 1: no such code), 4 code-length symbol.
+enum : uint32_t { E_LIT = 0, E_EOB = 1, E_DIST = 2, E_SPECIAL = 3, E_CL = 4 };
+constexpr uint16_t E_LONG = (uint16_t)(E_SPECIAL << 12);
+constexpr uint16_t E_BAD = (uint16_t)((E_SPECIAL << 12) | 1u);
+
+__device__ __forceinline__ uint32_t e_len(uint32_t e) { return (e >> 8) & 15u; }
+__device__ __forceinline__ uint32_t e_kind(uint32_t e) { return (e >> 12) & 7u; }
+
+// RFC 1951 3.2.5 in closed form: length symbol i = sym - 257 (0-28), distance symbol i (0-29).
+__device__ __forceinline__ void len_code(uint32_t i, uint32_t& base, uint32_t& ext) {
+    if (i < 4) {
+        base = 3 + i;
+        ext = 0;
+    } else if (i == 28) {
+        base = 258;
+        ext = 0;
+    } else {
+        ext = (i >> 2) - 1;
+        base = 3 + ((4u | (i & 3u)) << ext);
+    }
+}
+__device__ __forceinline__ void dist_code(uint32_t i, uint32_t& base, uint32_t& ext) {
+    if (i < 4) {
+        base = 1 + i;
+        ext = 0;
+    } else {
+        ext = (i >> 1) - 1;
+        base = 1 + ((2u | (i & 1u)) << ext);
+    }
+}
+
+// RFC 1951 3.2.7: order of the code length code lengths.
+__constant__ uint8_t kClOrder[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+
+enum : int { T_CL = 0, T_LIT = 1, T_DIST = 2 };
+
+__device__ __forceinline__ uint16_t sym_entry(int kind, uint32_t s, uint32_t L) {
+    if (kind == T_CL) return (uint16_t)((E_CL << 12) | (L << 8) | s);
+    if (kind == T_LIT) {
+        if (s < 256) return (uint16_t)((L << 8) | s);
+        if (s == 256) return (uint16_t)((E_EOB << 12) | (L << 8));
+        if (s < 286) {
+            uint32_t base, ext;
+            len_code(s - 257, base, ext);
+            return (uint16_t)(0x8000u | (ext << 12) | (L << 8) | (base - 3));
+        }
+        return E_BAD;
+    }
+    if (s < 30) return (uint16_t)((E_DIST << 12) | (L << 8) | s);
+    return E_BAD;
+}
+
+// 16-bit units (the token arena): a literal 0x00bb; a match head 0x8000 | (length - 3) << 6 |
+// (distance - 1) >> 9, followed by its tail 0xC000 | ((distance - 1) & 0x1FF).
+__device__ __forceinline__ uint32_t unit_match(uint32_t len, uint32_t dist) {
+    const uint32_t d = dist - 1;
+    return (0x8000u | ((len - 3) << 6) | (d >> 9)) | ((0xC000u | (d & 0x1FFu)) << 16);
+}
+
+// Workspace: [0, 256) queue counters; per job (units, status) as two u32; the arena after that,
+// 256-byte aligned.
+constexpr size_t WS_HEAD = 256;
+__host__ __device__ __forceinline__ size_t arena_offset(long long n_jobs) {
+    return (WS_HEAD + 8 * (size_t)n_jobs + 255) & ~(size_t)255;
+}
+// Byte offset of job j's slot in the arena (8-byte aligned; 2 ISIZE + 8 bytes long).
+__device__ __forceinline__ unsigned long long slot_of_job(long long out_off, long long j) {
+    return ((unsigned long long)(2 * out_off + 16 * j) + 7ull) & ~7ull;
+}
+
+// ---------------------------------------------------------------- k_decode: one member per lane
+
+template <int LB_, int DB_, int WARPS_>
+struct DecCfg {
+    static constexpr int LB = LB_, DB = DB_, WARPS = WARPS_;
+    static constexpr int NLL = 15 - LB_, NLD = 15 - DB_;  // code lengths longer than the roots
+    static constexpr uint32_t LMASK = (1u << LB_) - 1, DMASK = (1u << DB_) - 1;
+    // the lane's literal/length table holds its code lengths while a dynamic header is read (up to
+    // 286 + 30 bytes); its distance table holds the code-length code's table (2^7 entries)
+    static_assert((2 << LB_) >= 320 && DB_ >= 7 && NLL <= 8 && NLD <= 8, "table sizes");
+    struct WarpSmem {
+        uint16_t lit[32][1 << LB_];
+        uint16_t dist[32][1 << DB_];
+        uint16_t lsym[32][288];    // entries of the literal/length codes longer than LB, canonical order
+        uint16_t dsym[32][32];     // entries of the distance codes longer than DB
+        uint8_t lens[320];         // the code lengths of the lane whose tables the warp builds
+        uint32_t scratch[48];
+        uint32_t lim[16];          // limits computed for that lane: NLL literal/length, then NLD distance
+    };
+    struct CtaSmem {
+        WarpSmem w[WARPS_];
+    };
+};
+
+enum : int { S_IDLE = 0, S_HDR = 1, S_BUILD_CL = 2, S_CLENS = 3, S_BUILD = 4, S_RUN = 5, S_STORED = 6, S_FIN = 7,
+             S_DONE = 8 };
+
+// Canonical table of lens[0:nsym) for one lane, built by the whole warp: tab[2^lb] indexed by the
+// next lb bits (LSB first); codes longer than lb bits have their entries in sym[] in canonical
+// order and, for code length lb + 1 + i, lim[i] = (end of the length's codes, left-justified to 15
+// bits) | (index in sym[] of its first code minus that code) << 16.  Acceptance as zlib's inflate:
+// an over-subscribed code is an error; an incomplete one too, except a literal/length or distance
+// code whose longest code has length 1 (the code-length code must be complete).  Returns false on
+// error (the same in every lane).
+__device__ __noinline__ bool build_lane(const uint8_t* lens, int nsym, int lb, int kind, uint16_t* tab, uint32_t* lim,
+                                        uint16_t* sym, uint32_t* scratch) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 16) scratch[lane] = 0;
+    __syncwarp();
+    for (int s = lane; s < nsym; s += 32) {
+        const uint32_t L = lens[s];
+        if (L) atomicAdd(&scratch[L], 1u);
+    }
+    __syncwarp();
+    const uint32_t cnt = (lane >= 1 && lane < 16) ? scratch[lane] : 0u;
+    int left = 1, maxlen = 0;
+    uint32_t code = 0, index = 0, my_first = 0, my_index = 0;
+    for (int L = 1; L < 16; L++) {
+        const uint32_t c = __shfl_sync(FULL, cnt, L);
+        left = (left << 1) - (int)c;
+        if (c) maxlen = L;
+        if (lane == L) {
+            my_first = code;
+            my_index = index;
+        }
+        index += c;
+        code = (code + c) << 1;
+        if (left < 0) break;
+    }
+    __syncwarp();
+    if (left < 0) return false;
+    const bool incomplete = left > 0;
+    if (kind == T_CL && (incomplete || maxlen == 0)) return false;
+    if (incomplete && maxlen > 1) return false;
+    const uint32_t nshort = __shfl_sync(FULL, my_index, lb < 15 ? lb + 1 : 15);
+    if (lim && lane > lb && lane < 16) {
+        const uint32_t limit = (my_first + cnt) << (15 - lane);
+        const int base = (int)(my_index - nshort) - (int)my_first;
+        lim[lane - lb - 1] = (limit & 0xFFFFu) | ((uint32_t)(uint16_t)(int16_t)base << 16);
+    }
+    if (lane >= 1 && lane < 16) {
+        scratch[lane] = my_index;        // running insertion index of the length
+        scratch[16 + lane] = my_first;   // first code of the length
+        scratch[32 + lane] = my_index;   // first index of the length
+    }
+    // slots no code reaches (an incomplete code) decode as errors; complete codes cover every slot
+    if (incomplete || maxlen == 0)
+        for (int i = lane; i < (1 << lb); i += 32) tab[i] = E_BAD;
+    __syncwarp();
+    for (int base = 0; base < nsym; base += 32) {
+        const int s = base + lane;
+        const uint32_t L = s < nsym ? lens[s] : 0u;
+        const uint32_t peers = __match_any_sync(FULL, L);
+        const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+        const uint32_t pos = L ? scratch[L] : 0u;
+        __syncwarp();
+        if (L && lane == __ffs(peers) - 1) scratch[L] = pos + __popc(peers);
+        __syncwarp();
+        if (L) {
+            const uint32_t idx = pos + rank;
+            const uint32_t c = scratch[16 + L] + (idx - scratch[32 + L]);
+            const uint16_t e = sym_entry(kind, (uint32_t)s, L);
+            if ((int)L <= lb) {
+                const uint32_t r = __brev(c) >> (32 - L);
+                for (uint32_t x = r; x < (1u << lb); x += (1u << L)) tab[x] = e;
+            } else {
+                sym[idx - nshort] = e;
+                tab[__brev(c >> (L - lb)) >> (32 - lb)] = E_LONG;
+            }
+        }
+        __syncwarp();
+    }
+    return true;
+}
+
+// The entry of a code longer than the root bits from the lane's limits: x holds the next 15+ bits.
+template <int N, int NSYM>
+__device__ __forceinline__ uint32_t long_entry(uint32_t x, const uint32_t (&lim)[N], const uint16_t* sym) {
+    const uint32_t c = __brev(x) >> 17;  // the next 15 bits, first bit highest
+    int idx = -1;
+#pragma unroll
+    for (int i = N - 1; i >= 0; i--)
+        if (c < (lim[i] & 0xFFFFu)) idx = (int)(int16_t)(lim[i] >> 16) + (int)(c >> (N - 1 - i));
+    return (idx >= 0 && idx < NSYM) ? (uint32_t)sym[idx] : (uint32_t)E_BAD;
+}
+
+__device__ __forceinline__ void report(cb_inflate_summary* summary, uint32_t* job_status, long long j, uint32_t st) {
+    if (job_status) job_status[j] = st;
+    if (st != CB_OK) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&summary->n_bad), 1ull);
+        atomicMin(reinterpret_cast<long long*>(&summary->first_bad), j);
+        atomicMax(&summary->status, (int)st);
+    }
+}
+
+__device__ __forceinline__ uint32_t load_word(const uint32_t* wbase, uint32_t nvalid, uint32_t w) {
+    return w < nvalid ? __ldg(wbase + w) : 0u;
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::WARPS * 32)
+    k_decode(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
+             uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes,
+             int steps) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    typename C::CtaSmem& S = *reinterpret_cast<typename C::CtaSmem*>(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    typename C::WarpSmem& W = S.w[warp];
+    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws);
+    uint32_t* per_job = reinterpret_cast<uint32_t*>(ws + WS_HEAD);  // (units, status) per job
+    uint8_t* arena = ws + arena_offset(n_jobs);
+    long long n = n_jobs;
+    if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
+
+    uint16_t* my_lit = W.lit[lane];
+    uint16_t* my_dist = W.dist[lane];
+    uint8_t* my_lens = reinterpret_cast<uint8_t*>(my_lit);  // code lengths while a header is read
+
+    // the member of this lane
+    int st = S_IDLE;
+    long long j = 0;
+    const uint32_t* wbase = nullptr;
+    uint32_t nvalid = 0, w = 0, lo = 0, hi = 0, off = 0;  // bit reader: lo = word w, hi = word w + 1
+    uint32_t s0 = 0, in_bits = 0, isize = 0, pos = 0;
+    bool final_block = false;
+    uint32_t rem = 0, hlit = 0, total = 0, ci = 0;  // stored bytes left; code lengths read
+    uint64_t* slot = nullptr;
+    uint32_t nunits = 0, nq = 0, pcnt = 0;           // units written, u64 groups stored, units pending
+    uint64_t pend = 0;
+    uint32_t err = CB_OK;
+    uint32_t llim[C::NLL], dlim[C::NLD];
+#pragma unroll
+    for (int i = 0; i < C::NLL; i++) llim[i] = 0;
+#pragma unroll
+    for (int i = 0; i < C::NLD; i++) dlim[i] = 0;
+
+    auto adv = [&](uint32_t k) {  // k <= 32
+        off += k;
+        if (off >= 32) {
+            off -= 32;
+            w++;
+            lo = hi;
+            hi = load_word(wbase, nvalid, w + 1);
+        }
+    };
+    auto window = [&]() { return __funnelshift_r(lo, hi, off); };
+    auto consumed = [&]() { return w * 32u + off - s0; };
+    auto put = [&](uint32_t v, uint32_t k) {  // append k (1 or 2) units, packed low unit first
+        const uint32_t c = pcnt;
+        pend |= (uint64_t)v << (16 * c);
+        pcnt = c + k;
+        nunits += k;
+        if (pcnt >= 4) {
+            slot[nq++] = pend;
+            pend = pcnt > 4 ? (uint64_t)(v >> 16) : 0ull;
+            pcnt -= 4;
+        }
+    };
+    auto fail = [&](uint32_t code) {
+        err = code;
+        st = S_FIN;
+    };
+
+    for (;;) {
+        // ---- lanes without a member take the next ones (one atomic per warp)
+        const unsigned idle = __ballot_sync(FULL, st == S_IDLE);
+        if (idle) {
+            const int leader = __ffs(idle) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (st == S_IDLE) {
+                j = (long long)base + __popc(idle & ((1u << lane) - 1u));
+                if (j >= n) {
+                    st = S_DONE;
+                } else {
+                    const cb_member_job job = jobs[j];
+                    const uintptr_t in = (uintptr_t)job.in;
+                    wbase = reinterpret_cast<const uint32_t*>(in & ~(uintptr_t)3);
+                    s0 = (uint32_t)(in & 3) * 8;
+                    nvalid = (uint32_t)((in + job.in_len + 8 - (uintptr_t)wbase) >> 2);
+                    in_bits = job.in_len * 8u;
+                    isize = job.isize;
+                    w = 0;
+                    off = s0;
+                    lo = load_word(wbase, nvalid, 0);
+                    hi = load_word(wbase, nvalid, 1);
+                    pos = 0;
+                    final_block = false;
+                    nunits = nq = pcnt = 0;
+                    pend = 0;
+                    err = CB_OK;
+                    st = S_HDR;
+                    const unsigned long long so = slot_of_job(job.out_off, j);
+                    slot = reinterpret_cast<uint64_t*>(arena + so);
+                    if (job.out_off < 0 || so + 2ull * isize + 8ull > arena_bytes) fail(CB_ERR_CAPACITY);
+                    // slots are disjoint only for jobs in increasing out_off with disjoint outputs
+                    else if (j + 1 < n && jobs[j + 1].out_off < job.out_off + (long long)isize) fail(CB_ERR_ARG);
+                }
+            }
+        }
+        if (__all_sync(FULL, st == S_DONE)) break;
+
+        // ---- code tables, built by the whole warp for one lane at a time
+        for (unsigned b = __ballot_sync(FULL, st == S_BUILD_CL || st == S_BUILD); b; b &= b - 1) {
+            const int t = __ffs(b) - 1;
+            const int tst = __shfl_sync(FULL, st, t);
+            bool ok;
+            if (tst == S_BUILD_CL) {
+                // the code-length code: lengths in lane t's first 19 bytes, table into its distance table
+                const uint8_t* tl = reinterpret_cast<const uint8_t*>(W.lit[t]);
+                if (lane < 19) W.lens[lane] = tl[lane];
+                __syncwarp();
+                ok = build_lane(W.lens, 19, 7, T_CL, W.dist[t], nullptr, nullptr, W.scratch);
+            } else {
+                // literal/length and distance codes: fixed (hlit 0 marks a fixed block) or lane t's lengths
+                const uint32_t th = __shfl_sync(FULL, hlit, t);
+                const uint32_t ttot = __shfl_sync(FULL, total, t);
+                int nl, nd;
+                if (th == 0) {
+                    for (int s = lane; s < 320; s += 32)
+                        W.lens[s] = s < 144 ? 8 : s < 256 ? 9 : s < 280 ? 7 : s < 288 ? 8 : 5;
+                    nl = 288;
+                    nd = 32;
+                } else {
+                    const uint8_t* tl = reinterpret_cast<const uint8_t*>(W.lit[t]);
+                    for (uint32_t s = lane; s < ttot; s += 32) W.lens[s] = tl[s];
+                    nl = (int)th;
+                    nd = (int)(ttot - th);
+                }
+                __syncwarp();
+                ok = build_lane(W.lens, nl, C::LB, T_LIT, W.lit[t], W.lim, W.lsym[t], W.scratch) &&
+                     build_lane(W.lens + nl, nd, C::DB, T_DIST, W.dist[t], W.lim + C::NLL, W.dsym[t], W.scratch);
+            }
+            __syncwarp();
+            if (lane == t) {
+                if (!ok) {
+                    fail(CB_ERR_INFLATE);
+                } else if (tst == S_BUILD_CL) {
+                    st = S_CLENS;
+                    ci = 0;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < C::NLL; i++) llim[i] = W.lim[i];
+#pragma unroll
+                    for (int i = 0; i < C::NLD; i++) dlim[i] = W.lim[C::NLL + i];
+                    st = S_RUN;
+                }
+            }
+            __syncwarp();
+        }
+
+        // ---- block headers and member ends (each lane its own; rare)
+        if (st == S_HDR) {
+            if (consumed() > in_bits) {
+                fail(CB_ERR_INFLATE);
+            } else {
+                uint32_t x = window();
+                const uint32_t h = x & 7u;
+                adv(3);
+                final_block = (h & 1u) != 0;
+                const uint32_t btype = h >> 1;
+                if (btype == 0) {
+                    adv((8u - (off & 7u)) & 7u);  // to a byte boundary (the payload starts on one)
+                    x = window();
+                    const uint32_t len = x & 0xFFFFu, nlen = x >> 16;
+                    adv(16);
+                    adv(16);
+                    if (len != (~nlen & 0xFFFFu) || len > isize - pos || consumed() + 8ull * len > in_bits) {
+                        fail(CB_ERR_INFLATE);
+                    } else {
+                        rem = len;
+                        st = len ? S_STORED : (final_block ? S_FIN : S_HDR);
+                    }
+                } else if (btype == 1) {
+                    hlit = 0;  // fixed codes
+                    st = S_BUILD;
+                } else if (btype == 2) {
+                    x = window();
+                    hlit = (x & 31u) + 257;
+                    const uint32_t hdist = ((x >> 5) & 31u) + 1, hclen = ((x >> 10) & 15u) + 4;
+                    adv(14);
+                    if (hlit > 286 || hdist > 30) {
+                        fail(CB_ERR_INFLATE);
+                    } else {
+                        total = hlit + hdist;
+                        uint32_t* z = reinterpret_cast<uint32_t*>(my_lens);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) z[k] = 0;
+                        for (uint32_t i = 0; i < hclen; i++) {
+                            my_lens[kClOrder[i]] = (uint8_t)(window() & 7u);
+                            adv(3);
+                        }
+                        st = S_BUILD_CL;
+                    }
+                } else {
+                    fail(CB_ERR_INFLATE);
+                }
+            }
+        }
+        if (st == S_FIN) {
+            if (err == CB_OK && (consumed() > in_bits || pos != isize)) err = CB_ERR_INFLATE;
+            if (err == CB_OK && pcnt) slot[nq] = pend;  // the last units (the slot has 8 spare bytes)
+            per_job[2 * j] = nunits;
+            per_job[2 * j + 1] = err;
+            report(summary, job_status, j, err);
+            st = S_IDLE;
+        }
+
+        // ---- decode steps (lock step over the lanes' own streams)
+#pragma unroll 1
+        for (int k = 0; k < steps; k++) {
+            if (st == S_RUN) {
+                const uint32_t x = window();
+                uint32_t e = my_lit[x & C::LMASK];
+                if (e == E_LONG) e = long_entry<C::NLL, 288>(x, llim, W.lsym[lane]);
+                const uint32_t L = e_len(e);
+                if (e & 0x8000u) {
+                    const uint32_t ext = (e >> 12) & 7u;
+                    const uint32_t len = (e & 255u) + 3 + ((x >> L) & ((1u << ext) - 1u));
+                    adv(L + ext);
+                    const uint32_t y = window();
+                    uint32_t d = my_dist[y & C::DMASK];
+                    if (d == E_LONG) d = long_entry<C::NLD, 32>(y, dlim, W.dsym[lane]);
+                    const uint32_t dl = e_len(d);
+                    uint32_t dbase, dext;
+                    dist_code(d & 31u, dbase, dext);
+                    const uint32_t dist = dbase + ((y >> dl) & ((1u << dext) - 1u));
+                    adv(dl + dext);
+                    if (e_kind(d) != E_DIST || (d & 0x8000u) || dist > pos || len > isize - pos) {
+                        fail(CB_ERR_INFLATE);
+                    } else {
+                        put(unit_match(len, dist), 2);
+                        pos += len;
+                    }
+                } else if (e < 0x1000u) {
+                    adv(L);
+                    if (pos >= isize) {
+                        fail(CB_ERR_INFLATE);
+                    } else {
+                        put(e & 255u, 1);
+                        pos++;
+                    }
+                } else if (e_kind(e) == E_EOB) {
+                    adv(L);
+                    st = final_block ? S_FIN : S_HDR;
+                } else {
+                    fail(CB_ERR_INFLATE);
+                }
+            } else if (st == S_CLENS) {
+                const uint32_t x = window();
+                const uint32_t e = my_dist[x & 127u];
+                const uint32_t L = e_len(e), s = e & 255u;
+                if (e_kind(e) != E_CL || (e & 0x8000u) || L == 0) {
+                    fail(CB_ERR_INFLATE);
+                } else if (s < 16) {
+                    adv(L);
+                    my_lens[ci++] = (uint8_t)s;
+                } else {
+                    uint32_t rep, val = 0, eb;
+                    if (s == 16) {
+                        rep = 3 + ((x >> L) & 3u);
+                        eb = 2;
+                        val = ci ? my_lens[ci - 1] : 0u;
+                    } else if (s == 17) {
+                        rep = 3 + ((x >> L) & 7u);
+                        eb = 3;
+                    } else {
+                        rep = 11 + ((x >> L) & 127u);
+                        eb = 7;
+                    }
+                    adv(L + eb);
+                    if ((s == 16 && ci == 0) || ci + rep > total) {
+                        fail(CB_ERR_INFLATE);
+                    } else {
+                        for (uint32_t r = 0; r < rep; r++) my_lens[ci + r] = (uint8_t)val;
+                        ci += rep;
+                    }
+                }
+                if (st == S_CLENS && ci == total) {
+                    if (my_lens[256] == 0) fail(CB_ERR_INFLATE);  // no end-of-block code
+                    else st = S_BUILD;
+                }
+            } else if (st == S_STORED) {
+                const uint32_t x = window();
+                const uint32_t k2 = rem >= 2 ? 2u : 1u;
+                adv(8 * k2);
+                put(k2 == 2 ? ((x & 255u) | ((x << 8) & 0xFF0000u)) : (x & 255u), k2);
+                pos += k2;
+                rem -= k2;
+                if (rem == 0) st = final_block ? S_FIN : S_HDR;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- k_copy: one member per warp
+
+constexpr uint32_t RING = 32768;          // every DEFLATE distance reads the ring
+constexpr uint32_t RMASK = RING - 1;
+constexpr int WIN = 1024;                 // flush and CRC window
+static_assert(WIN == 32 * 32, "one 32-byte CRC column per lane");
+
+template <int WARPS_>
+struct CopyCfg {
+    static constexpr int WARPS = WARPS_;
+    struct CtaSmem {
+        uint32_t crc8[8][256];
+        uint32_t mulk[4][256];   // x * x^(8 (WIN - 32)) by bytes: moves a column past the other lanes
+        alignas(16) uint8_t ring[WARPS_][RING];
+    };
+};
+
+template <class S>
+__device__ __forceinline__ uint32_t mulk(const S& s, uint32_t x) {
+    return s.mulk[0][x & 255] ^ s.mulk[1][(x >> 8) & 255] ^ s.mulk[2][(x >> 16) & 255] ^ s.mulk[3][x >> 24];
+}
+
+// Store output bytes [ws, we) from the ring (byte p at slot p + a) to out, and fold them into this
+// lane's CRC column (window kwin; windows are aligned to the end of the member, the first one
+// padded by `pad` zero bytes in front).
+template <class S>
+__device__ __noinline__ uint32_t flush_window(uint8_t* out, uint32_t a, uint32_t ws, uint32_t we, uint32_t kwin,
+                                              uint32_t pad, uint32_t col, const uint8_t* ring, const S& s, bool crc) {
+    const int lane = threadIdx.x & 31;
+    const uintptr_t o16 = (uintptr_t)out & ~(uintptr_t)15;
+    const uintptr_t lo = (uintptr_t)out + ws, hi = (uintptr_t)out + we;
+    const uintptr_t A0 = lo & ~(uintptr_t)15;
+    const uint32_t nunits = (uint32_t)(((hi + 15) & ~(uintptr_t)15) - A0) >> 4;
+    for (uint32_t u = lane; u < nunits; u += 32) {
+        const uintptr_t ga = A0 + 16 * (uintptr_t)u;
+        const uint32_t sl = (uint32_t)(ga - o16) & RMASK;
+        if (ga >= lo && ga + 16 <= hi) {
+            *reinterpret_cast<uint4*>(ga) = *reinterpret_cast<const uint4*>(ring + sl);
+        } else {
+            for (uint32_t k = 0; k < 16; k++)
+                if (ga + k >= lo && ga + k < hi) *reinterpret_cast<uint8_t*>(ga + k) = ring[(sl + k) & RMASK];
+        }
+    }
+    if (crc) {
+        uint32_t c = mulk(s, col);
+        const long long v0 = (long long)kwin * WIN + 32 * lane - (long long)pad;  // position of the column
+#pragma unroll
+        for (int q = 0; q < 32; q += 8) {
+            uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const long long r0 = v0 + q + t, r1 = v0 + q + 4 + t;
+                const uint32_t b0 = r0 >= 0 ? ring[(uint32_t)(r0 + a) & RMASK] : 0u;
+                const uint32_t b1 = r1 >= 0 ? ring[(uint32_t)(r1 + a) & RMASK] : 0u;
+                w0 |= b0 << (8 * t);
+                w1 |= b1 << (8 * t);
+            }
+            c = crc_step8(s.crc8, c, w0, w1);
+        }
+        col = c;
+    }
+    __syncwarp();
+    return col;
+}
+
+// zlib's CRC32 of the member from the lane columns.
+__device__ __noinline__ uint32_t finish_crc(uint32_t col, uint32_t isize) {
+    const int lane = threadIdx.x & 31;
+    uint32_t v = col;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const int d = 1 << k;
+        const uint32_t other = __shfl_down_sync(FULL, v, d);
+        if ((lane & (2 * d - 1)) == 0) v = gf_mul(v, kCrc.seg[k]) ^ other;
+    }
+    v = __shfl_sync(FULL, v, 0);
+    return crc_finish(v, isize);
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::WARPS * 32)
+    k_copy(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
+           uint8_t* out_base, int check_crc, uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    typename C::CtaSmem& S = *reinterpret_cast<typename C::CtaSmem*>(smem_raw);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) S.mulk[b][i] = gf_mul((uint32_t)i << (8 * b), kCrc.k992);
+    }
+    init_crc8(S.crc8);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint8_t* ring = S.ring[warp];
+    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + 1;
+    const uint32_t* per_job = reinterpret_cast<const uint32_t*>(ws + WS_HEAD);
+    const uint8_t* arena = ws + arena_offset(n_jobs);
+    long long n = n_jobs;
+    if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
+    const bool crc = check_crc != 0;
+
+    for (;;) {
+        unsigned long long jj = 0;
+        if (lane == 0) jj = atomicAdd(queue, 1ull);
+        const long long j = (long long)__shfl_sync(FULL, jj, 0);
+        if (j >= n) break;
+        if (per_job[2 * j + 1] != CB_OK) continue;  // k_decode reported it
+        const cb_member_job job = jobs[j];
+        const uint32_t nu = per_job[2 * j];
+        const uint16_t* U = reinterpret_cast<const uint16_t*>(arena + slot_of_job(job.out_off, j));
+        uint8_t* out = out_base + job.out_off;
+        const uint32_t a = (uint32_t)((uintptr_t)out & 15);
+        const uint32_t isize = job.isize;
+        const uint32_t pad = (uint32_t)(-(int32_t)isize) & (WIN - 1);
+        uint32_t p = 0, ws_ = 0, we = min((uint32_t)WIN - pad, isize), kwin = 0, col = 0;
+        uint32_t st = (nu > isize) ? (uint32_t)CB_ERR_INFLATE : (uint32_t)CB_OK;
+        uint32_t g = 0;
+        uint32_t u = ((uint32_t)lane < nu && st == CB_OK) ? (uint32_t)__ldcs(U + lane) : 0u;
+        while (st == CB_OK && g < nu) {
+            // this group: units [g, g + cnt); a match head in lane 31 waits for the next group
+            const uint32_t avail = min(32u, nu - g);
+            const uint32_t nxt = __shfl_down_sync(FULL, u, 1);
+            const bool head31 = avail == 32 && (__shfl_sync(FULL, u, 31) & 0xC000u) == 0x8000u;
+            const uint32_t cnt = avail - (head31 ? 1u : 0u);
+            const bool valid = (uint32_t)lane < cnt;
+            const bool is_lit = valid && !(u & 0x8000u);
+            const bool is_head = valid && (u & 0xC000u) == 0x8000u;
+            // a head's tail is the next unit of the group (a head at the end of the units is an error)
+            const bool bad_head = is_head && ((uint32_t)lane + 1 >= cnt || (nxt & 0xC000u) != 0xC000u);
+            const uint32_t len = is_lit ? 1u : is_head ? ((u >> 6) & 255u) + 3 : 0u;
+            const uint32_t dist = is_head ? ((((u & 63u) << 9) | (nxt & 511u)) + 1) : 0u;
+            // the next group's units are loaded while this one is written
+            const uint32_t g2 = g + cnt;
+            const uint32_t u2 = (g2 + lane < nu) ? (uint32_t)__ldcs(U + g2 + lane) : 0u;
+            uint32_t glen;
+            const uint32_t ex = warp_exclusive_scan(len, glen);
+            if (__any_sync(FULL, bad_head || (is_head && dist > p + ex)) || glen > isize - p) {
+                st = CB_ERR_INFLATE;
+                break;
+            }
+            // token word: literal byte, or 0x80000000 | distance
+            const uint32_t tw = is_head ? (0x80000000u | dist) : (u & 255u);
+            for (uint32_t r0 = 0; r0 < glen; r0 += 32) {
+                const uint32_t rel = r0 + lane;
+                // the token of byte rel: the last lane with ex <= rel (tails carry the next token's ex)
+                int k = 0;
+#pragma unroll
+                for (int step = 16; step; step >>= 1) {
+                    const int c = k + step;
+                    const uint32_t exc = __shfl_sync(FULL, ex, c & 31);
+                    if ((uint32_t)c < cnt && exc <= rel) k = c;
+                }
+                const uint32_t t = __shfl_sync(FULL, tw, k);
+                const uint32_t b = p + rel;
+                uint32_t val = t & 255u;
+                int src = lane;  // the lane of this round holding the byte's source
+                if (rel < glen && (t & 0x80000000u)) {
+                    const uint32_t x = b - (t & 0x7FFFFFFFu);
+                    if (x >= p + r0) src = (int)(x - (p + r0));
+                    else val = ring[(x + a) & RMASK];
+                }
+                bool need = src != lane;
+                for (int it = 0; it < 6 && __any_sync(FULL, need); it++) {
+                    const uint32_t v2 = __shfl_sync(FULL, val, src);
+                    const int s2 = __shfl_sync(FULL, src, src);
+                    const bool n2 = __shfl_sync(FULL, (int)need, src) != 0;
+                    if (need) {
+                        if (!n2) {
+                            val = v2;
+                            need = false;
+                        } else {
+                            src = s2;
+                        }
+                    }
+                }
+                if (rel < glen) ring[(b + a) & RMASK] = (uint8_t)val;
+                __syncwarp();
+            }
+            p += glen;
+            while (we > ws_ && p >= we) {
+                col = flush_window(out, a, ws_, we, kwin, pad, col, ring, S, crc);
+                ws_ = we;
+                we = min(we + WIN, isize);
+                kwin++;
+            }
+            g = g2;
+            u = u2;
+        }
+        if (st == CB_OK && p != isize) st = CB_ERR_INFLATE;
+        if (st == CB_OK && crc && finish_crc(col, isize) != job.crc) st = CB_ERR_CRC;
+        if (lane == 0 && st != CB_OK) report(summary, job_status, j, st);
+        __syncwarp();
+    }
+}
+
+__global__ void k_split_init(cb_inflate_summary* summary, unsigned long long* queue) {
+    summary->status = CB_OK;
+    summary->reserved = 0;
+    summary->n_bad = 0;
+    summary->first_bad = INT64_MAX;
+    queue[0] = 0;
+    queue[1] = 0;
+}
+
+__global__ void k_split_finish(cb_inflate_summary* summary) {
+    if (summary->first_bad == INT64_MAX) summary->first_bad = -1;
+}
+
+}  // namespace split
+}  // namespace cb
+
+using namespace cb;
+
+int cb_set_error(cudaError_t e);  // abi.cu
+
+namespace {
+
+constexpr int MAX_DEVICES = 64;
+
+// CTAs per SM of a kernel on the current device, setting its shared memory size once per device.
+template <class K>
+int occupancy(int (&cache)[MAX_DEVICES], K kernel, int threads, size_t smem) {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= MAX_DEVICES) return -1;
+    int& b = cache[d];
+    if (b > 0) return b;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int occ = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
+    if (e != cudaSuccess) return -(int)e;
+    b = occ > 0 ? occ : 1;
+    return b;
+}
+
+int fail_occ(int o) { return cb_set_error(o == -1 ? cudaErrorInvalidDevice : (cudaError_t)(-o)); }
+
+template <class D>
+int launch_decode(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint32_t* job_status,
+                  cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes, cudaStream_t s) {
+    static int cache[MAX_DEVICES];
+    const size_t smem = sizeof(typename D::CtaSmem);
+    const int o = occupancy(cache, split::k_decode<D>, D::WARPS * 32, smem);
+    if (o <= 0) return fail_occ(o);
+    long long grid = (long long)cb_device_sm_count() * o;
+    const long long by_work = (n_jobs + 32 * D::WARPS - 1) / (32 * D::WARPS);
+    if (!d_n_jobs && by_work < grid) grid = by_work;
+    split::k_decode<D><<<(unsigned)(grid < 1 ? 1 : grid), D::WARPS * 32, smem, s>>>(
+        jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, (int)cb_param(CB_PARAM_DECODE_STEPS));
+    return CB_OK;
+}
+
+template <class C>
+int launch_copy(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
+                uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, cudaStream_t s) {
+    static int cache[MAX_DEVICES];
+    const size_t smem = sizeof(typename C::CtaSmem);
+    const int o = occupancy(cache, split::k_copy<C>, C::WARPS * 32, smem);
+    if (o <= 0) return fail_occ(o);
+    long long grid = (long long)cb_device_sm_count() * o;
+    const long long by_work = (n_jobs + C::WARPS - 1) / C::WARPS;
+    if (!d_n_jobs && by_work < grid) grid = by_work;
+    split::k_copy<C><<<(unsigned)(grid < 1 ? 1 : grid), C::WARPS * 32, smem, s>>>(
+        jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws);
+    return CB_OK;
+}
+
+}  // namespace
+
+extern "C" size_t cb_inflate_split_workspace_bytes(int64_t n_jobs, int64_t out_bytes) {
+    if (n_jobs < 0 || out_bytes < 0) return 0;
+    return split::arena_offset(n_jobs) + 2 * (size_t)out_bytes + 16 * (size_t)n_jobs + 16;
+}
+
+extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
+                                int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+    if (!summary || !workspace || n_jobs < 0 || workspace_bytes < split::arena_offset(n_jobs) + 16) return CB_ERR_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint8_t* ws = reinterpret_cast<uint8_t*>(workspace);
+    const unsigned long long arena_bytes = workspace_bytes - split::arena_offset(n_jobs);
+    split::k_split_init<<<1, 1, 0, s>>>(summary, reinterpret_cast<unsigned long long*>(ws));
+    if (n_jobs > 0) {
+        const int rb = (int)cb_param(CB_PARAM_DECODE_ROOT);
+        int rc = rb == 9 ? launch_decode<split::DecCfg<9, 7, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws,
+                                                                 arena_bytes, s)
+                         : launch_decode<split::DecCfg<8, 7, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws,
+                                                                 arena_bytes, s);
+        if (rc != CB_OK) return rc;
+        const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
+        if (cw == 2)
+            rc = launch_copy<split::CopyCfg<2>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
+        else if (cw == 6)
+            rc = launch_copy<split::CopyCfg<6>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
+        else
+            rc = launch_copy<split::CopyCfg<3>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
+        if (rc != CB_OK) return rc;
+    }
+    split::k_split_finish<<<1, 1, 0, s>>>(summary);
+    return cb_set_error(cudaGetLastError());
+}

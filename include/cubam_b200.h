@@ -83,6 +83,28 @@ const char* cb_last_error(void);
 /* Number of SMs of the current device (for sizing persistent grids). */
 int cb_device_sm_count(void);
 
+/* ---- launch parameters (no counterpart in cubam, whose launch shapes are fixed:
+ *      src/cubam/_kernels.py:637-641, and whose chunk size is a fixed policy:
+ *      src/cubam/_memory.py:11-23) ---------------------------------------------------------------
+ * One value per key for the whole process, read by every later launch; the package's autotuner
+ * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
+ *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB (32 KiB)
+ *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (1)
+ *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 8 or 9 (8)
+ *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 (3)
+ *   CB_PARAM_DECODE_STEPS  decode steps of form 3 between lane scheduling rounds: 1-64 (16)
+ * cb_set_param(key, 0) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
+ * cb_get_param returns the current value, -1 for an unknown key. */
+enum {
+    CB_PARAM_CHAIN_TILE = 1,
+    CB_PARAM_INFLATE_FORM = 2,
+    CB_PARAM_DECODE_ROOT = 3,
+    CB_PARAM_COPY_WARPS = 4,
+    CB_PARAM_DECODE_STEPS = 5
+};
+int cb_set_param(int key, int64_t value);
+int64_t cb_get_param(int key);
+
 /* ---- BGZF member scan: replaces bgzf_candidates + bgzf_sizes + chain + the checks of _inflate_blocks
  *      (src/cubam/_kernels.py:69-89, src/cubam/_kernels.py:662-702, src/cubam/bgzf.py:542-586) ---------- */
 
@@ -119,28 +141,43 @@ int cb_scan_members_noalloc(const uint8_t* buf, int64_t n, int eof, int64_t out_
 /* ---- Inflate: replaces nvcompBatchedDeflateDecompressAsync and the status/size check
  *      (src/cubam/bgzf.py:587-611); adds the CRC32 check ---------------------------------------- */
 
-/* Workspace bytes of cb_inflate. */
+/* Workspace bytes of cb_inflate's forms 1 and 2 (form 3 takes cb_inflate_split_workspace_bytes). */
 size_t cb_inflate_workspace_bytes(void);
 
 /* Inflate jobs[0:n_jobs) (raw DEFLATE: stored, fixed and dynamic Huffman blocks) into
- * out_base + jobs[i].out_off with a persistent grid that takes members from a work queue.
+ * out_base + jobs[i].out_off with persistent grids that take members from a work queue.
  * When d_n_jobs is not NULL the job count is read from device memory (n_jobs is then the
  * capacity).  Each member must give exactly isize bytes; with check_crc its CRC32 must match.
- * job_status (device, may be NULL) gets a code per job.  Runs the one-member-per-warp form
- * (cb_inflate_form with form 1). */
+ * job_status (device, may be NULL) gets a code per job.  Runs cb_inflate_form with form 0: the
+ * form CB_PARAM_INFLATE_FORM names. */
 int cb_inflate(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
                uint32_t* job_status, cb_inflate_summary* summary, void* workspace, size_t workspace_bytes,
                void* stream);
 
 /* cb_inflate with the form given: 1 = one member per warp, 2 = one member per lane (most
- * members in flight), 0 = as cb_inflate.  Both forms give the same bytes and the same per-job
- * codes.  No cubam counterpart (cubam has one nvCOMP call, src/cubam/bgzf.py:595). */
+ * members in flight), 3 = cb_inflate_split, 0 = CB_PARAM_INFLATE_FORM.  Form 3 runs only with a
+ * workspace larger than cb_inflate_workspace_bytes() (sized by cb_inflate_split_workspace_bytes);
+ * with the small workspace form 1 runs in its place.  Every form gives the same bytes and the same
+ * per-job codes.  No cubam counterpart (cubam has one nvCOMP call, src/cubam/bgzf.py:595). */
 int cb_inflate_form(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
                     int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
                     size_t workspace_bytes, int form, void* stream);
 
 /* Members the one-member-per-lane form keeps in flight on the current device (0 on error). */
 int64_t cb_inflate_lane_slots(void);
+
+/* ---- Inflate, form 3: the Huffman decode and the copy as two kernels (same contract as cb_inflate,
+ *      replacing the same nvCOMP call, src/cubam/bgzf.py:587-611) ---------------------------------
+ * k_decode decodes one member per lane (32 members per warp in lock step) into 16-bit units in a
+ * token arena inside the workspace; k_copy writes each member with one warp through a 32 KiB
+ * shared-memory window and checks its CRC32.  Jobs must have increasing out_off with disjoint
+ * outputs (as cb_scan_members writes them); a job out of that order fails with CB_ERR_ARG, a job
+ * whose arena slot does not fit the workspace with CB_ERR_CAPACITY.  out_bytes: an upper bound of
+ * out_off + isize over the jobs (the size of out_base's buffer). */
+size_t cb_inflate_split_workspace_bytes(int64_t n_jobs, int64_t out_bytes);
+int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
+                     int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
+                     size_t workspace_bytes, void* stream);
 
 /* ---- Record chain: replaces record_candidates + record_ends + chain (src/cubam/_kernels.py:250-289,
  *      src/cubam/bam.py:403-418) --------------------------------------------------------------- */

@@ -46,3 +46,22 @@ def test_bad_arguments_are_rejected_without_a_launch():
     assert _lib.lib.cb_inflate(None, -1, None, None, 1, None, None, None, 0, None) == _lib.ARG
     assert _lib.lib.cb_find_tags(None, None, 1, b"CB", 0, None, None, None, None, None) == _lib.ARG
     assert _lib.lib.cb_decode_fixed(None, None, -5, *([None] * 11), None) == _lib.ARG
+
+
+def test_launch_parameters_are_checked_and_restored():
+    from cubam_b200 import _lib
+
+    L = _lib.lib
+    assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 32768
+    assert L.cb_get_param(99) == -1
+    assert L.cb_set_param(99, 1) == _lib.ARG
+    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 3000) == _lib.ARG  # not a power of two
+    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 1 << 23) == _lib.ARG
+    assert L.cb_set_param(_lib.PARAM_COPY_WARPS, 4) == _lib.ARG
+    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 8192) == _lib.OK
+    assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 8192
+    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 0) == _lib.OK
+    assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 32768
+    for key, default in ((_lib.PARAM_INFLATE_FORM, 1), (_lib.PARAM_DECODE_ROOT, 8), (_lib.PARAM_COPY_WARPS, 3),
+                         (_lib.PARAM_DECODE_STEPS, 16)):
+        assert L.cb_get_param(key) == default

@@ -170,7 +170,7 @@ def _payloads(seed: int):
     return out
 
 
-FORMS = [1, 2]  # one member per warp, one member per lane
+FORMS = [1, 2, 3]  # one member per warp, one member per lane, decode per lane + copy per warp
 
 
 @pytest.mark.parametrize("form", FORMS)
@@ -255,9 +255,9 @@ def test_inflate_corrupt_members_are_errors(form):
     assert G._lib.INFLATE in seen
 
 
-def test_inflate_many_members_both_forms_same_codes():
-    """More members than the lane form has lanes, so lanes take member after member; some members
-    damaged.  Both forms give the payloads of the good members and the same per-job codes."""
+def test_inflate_many_members_all_forms_same_codes():
+    """More members than the lane forms have lanes, so lanes take member after member; some members
+    damaged.  Every form gives the payloads of the good members and the same per-job codes."""
     rng = random.Random(11)
     nrng = np.random.default_rng(11)
     n = int(G._lib.lib.cb_inflate_lane_slots()) + 3000
@@ -287,15 +287,16 @@ def test_inflate_many_members_both_forms_same_codes():
         assert (codes != 99).all()
         assert int(summ.n_bad) == int((codes != 0).sum())
         results.append((_np(out).tobytes(), codes))
-    (out1, codes1), (out2, codes2) = results
-    assert (codes1 == codes2).all()
+    codes1 = results[0][1]
+    for _, codes in results[1:]:
+        assert (codes1 == codes).all()
     assert set(np.flatnonzero(codes1)) <= bad
     offs = np.cumsum([0] + [len(p) for p in payloads])
     good = np.flatnonzero(codes1 == 0)
     assert len(good) >= n - len(bad)
     for i in good[:: max(1, len(good) // 2000)].tolist() + good[-50:].tolist():
-        assert out1[offs[i]:offs[i + 1]] == payloads[i], i
-        assert out2[offs[i]:offs[i + 1]] == payloads[i], i
+        for out, _ in results:
+            assert out[offs[i]:offs[i + 1]] == payloads[i], i
 
 
 def test_records_cross_members_and_chunks(tmp_path):
