@@ -32,9 +32,10 @@ struct Param {
 constexpr Param kParams[] = {
     {CB_PARAM_CHAIN_TILE, 2048, 1 << 22, 32768},
     {CB_PARAM_INFLATE_FORM, 1, 3, 1},
-    {CB_PARAM_DECODE_ROOT, 8, 9, 8},
-    {CB_PARAM_COPY_WARPS, 1, 6, 3},
+    {CB_PARAM_DECODE_ROOT, 6, 8, 7},
+    {CB_PARAM_COPY_WARPS, 2, 24, 12},
     {CB_PARAM_DECODE_STEPS, 1, 64, 16},
+    {CB_PARAM_DECODE_PREFETCH, 0, 16, 4},
 };
 constexpr int kNParams = sizeof(kParams) / sizeof(kParams[0]);
 std::atomic<int64_t> g_param[kNParams] = {};
@@ -58,7 +59,7 @@ extern "C" int64_t cb_get_param(int key) { return param_index(key) < 0 ? -1 : cb
 extern "C" int cb_set_param(int key, int64_t value) {
     const int i = param_index(key);
     if (i < 0) return cb_set_error_text(CB_ERR_ARG, "cb_set_param: unknown key");
-    if (value == 0) {  // back to the default
+    if (value == -1) {  // back to the default
         g_param_set[i].store(false, std::memory_order_release);
         return CB_OK;
     }
@@ -66,8 +67,8 @@ extern "C" int cb_set_param(int key, int64_t value) {
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
     if (key == CB_PARAM_CHAIN_TILE && (value & (value - 1)))
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is a power of two");
-    if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6)
-        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3 or 6");
+    if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6 && value != 12 && value != 24)
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3, 6, 12 or 24");
     g_param[i].store(value, std::memory_order_relaxed);
     g_param_set[i].store(true, std::memory_order_release);
     return CB_OK;

@@ -12,15 +12,20 @@
 //
 //  1. k_decode: one member per LANE.  32 members per warp advance one symbol per step in lock step,
 //     each lane with its own tables in shared memory (16-bit entries, 2^LB literal/length and 2^DB
-//     distance root entries; longer codes by per-length limits kept in registers), and write the
+//     distance root entries; longer codes by per-length limits kept in registers).  A step is one
+//     straight path for literals and matches alike (the warp pays for every path a lane takes, so
+//     they are merged and predicated), with a 64-bit bit buffer fed from two prefetched words, and
+//     writes the
 //     symbols as 16-bit units to a token arena in HBM: a literal is one unit, a match two (length and
 //     the high distance bits, then the low distance bits).  Block headers, code lengths and stored
 //     blocks are steps of the same lock-step loop; the code tables of one lane are built by the
 //     whole warp.  The output size, distances and the end of the payload are checked here.
 //  2. k_copy: one member per WARP.  The warp reads its member's units 32 at a time, places them by
-//     a prefix sum of their lengths, and writes the bytes 32 at a time into a 32 KiB ring in shared
-//     memory (every DEFLATE distance reads the ring); a byte whose source lies in the same 32 bytes
-//     takes it from another lane.  Completed 1 KiB windows go to HBM with 16-byte stores and into
+//     a prefix sum of their lengths, and writes the bytes 32 at a time into a 16 KiB ring in shared
+//     memory (sources up to about 16 KiB back; older ones, about one match in eight on the GEX-shaped
+//     workload, read the output already written to HBM); a byte finds its token from a bit mask of the
+//     tokens that start in its 32 bytes (one warp OR-reduction and a population count), and a byte
+//     whose source lies in the same 32 bytes takes it from another lane.  Completed 1 KiB windows go to HBM with 16-byte stores and into
 //     the CRC32 (32 lane columns joined in GF(2)).
 //
 // Units are at most one per output byte, so a member's units take at most 2 ISIZE bytes: the arena
@@ -121,17 +126,25 @@ struct DecCfg {
     static constexpr int LB = LB_, DB = DB_, WARPS = WARPS_;
     static constexpr int NLL = 15 - LB_, NLD = 15 - DB_;  // code lengths longer than the roots
     static constexpr uint32_t LMASK = (1u << LB_) - 1, DMASK = (1u << DB_) - 1;
-    // the lane's literal/length table holds its code lengths while a dynamic header is read (up to
-    // 286 + 30 bytes); its distance table holds the code-length code's table (2^7 entries)
-    static_assert((2 << LB_) >= 320 && DB_ >= 7 && NLL <= 8 && NLD <= 8, "table sizes");
+    // One region per lane (bytes):
+    //   LIT   u16[2^LB]  literal/length root entries
+    //   DIST  u16[2^DB]  distance root entries
+    //   DSYM  u16[32]    entries of the distance codes longer than DB, canonical order
+    //   LSYM  u8[288]    low 8 bits of the symbols of literal/length codes longer than LB, canonical order
+    //   LHI   u32[9]     bit i: symbol i of LSYM is 256 or more
+    // While the lane reads a dynamic header: the code-length code's table (u16[128]) at 0, the
+    // code lengths (up to 286 + 30 bytes) at LSYM, where the 19 lengths of the code-length code
+    // wait first.
+    static constexpr int LIT = 0, DIST = LIT + (2 << LB_), DSYM = DIST + (2 << DB_);
+    static constexpr int LSYM = DSYM + 64 > 256 ? DSYM + 64 : 256;
+    static constexpr int LHI = LSYM + 288;
+    static constexpr int STRIDE = (LHI + 36 + 7) & ~7;
+    static_assert(LSYM + 320 <= STRIDE && NLL <= 9 && NLD <= 10 && LB_ >= 5 && DB_ >= 4, "table sizes");
     struct WarpSmem {
-        uint16_t lit[32][1 << LB_];
-        uint16_t dist[32][1 << DB_];
-        uint16_t lsym[32][288];    // entries of the literal/length codes longer than LB, canonical order
-        uint16_t dsym[32][32];     // entries of the distance codes longer than DB
+        alignas(16) uint8_t lane[32][STRIDE];
         uint8_t lens[320];         // the code lengths of the lane whose tables the warp builds
         uint32_t scratch[48];
-        uint32_t lim[16];          // limits computed for that lane: NLL literal/length, then NLD distance
+        uint32_t lim[20];          // limits computed for that lane: NLL literal/length, then NLD distance
     };
     struct CtaSmem {
         WarpSmem w[WARPS_];
@@ -149,9 +162,10 @@ enum : int { S_IDLE = 0, S_HDR = 1, S_BUILD_CL = 2, S_CLENS = 3, S_BUILD = 4, S_
 // code whose longest code has length 1 (the code-length code must be complete).  Returns false on
 // error (the same in every lane).
 __device__ __noinline__ bool build_lane(const uint8_t* lens, int nsym, int lb, int kind, uint16_t* tab, uint32_t* lim,
-                                        uint16_t* sym, uint32_t* scratch) {
+                                        uint16_t* sym, uint8_t* sym8, uint32_t* hi8, uint32_t* scratch) {
     const int lane = threadIdx.x & 31;
     if (lane < 16) scratch[lane] = 0;
+    if (hi8 && lane < 9) hi8[lane] = 0;
     __syncwarp();
     for (int s = lane; s < nsym; s += 32) {
         const uint32_t L = lens[s];
@@ -210,7 +224,13 @@ __device__ __noinline__ bool build_lane(const uint8_t* lens, int nsym, int lb, i
                 const uint32_t r = __brev(c) >> (32 - L);
                 for (uint32_t x = r; x < (1u << lb); x += (1u << L)) tab[x] = e;
             } else {
-                sym[idx - nshort] = e;
+                const uint32_t li = idx - nshort;
+                if (sym8) {  // literal/length: the symbol's low byte, and a bit for 256 and up
+                    sym8[li] = (uint8_t)s;
+                    if (s >= 256) atomicOr(&hi8[li >> 5], 1u << (li & 31));
+                } else {
+                    sym[li] = e;
+                }
                 tab[__brev(c >> (L - lb)) >> (32 - lb)] = E_LONG;
             }
         }
@@ -230,6 +250,25 @@ __device__ __forceinline__ uint32_t long_entry(uint32_t x, const uint32_t (&lim)
     return (idx >= 0 && idx < NSYM) ? (uint32_t)sym[idx] : (uint32_t)E_BAD;
 }
 
+// The same for literal/length codes, whose long-code symbols are kept as a low byte and a high bit.
+template <int N>
+__device__ __forceinline__ uint32_t long_lit_entry(uint32_t x, const uint32_t (&lim)[N], const uint8_t* sym8,
+                                                   const uint32_t* hi8) {
+    const uint32_t c = __brev(x) >> 17;  // the next 15 bits, first bit highest
+    int idx = -1;
+    uint32_t L = 0;
+#pragma unroll
+    for (int i = N - 1; i >= 0; i--) {
+        if (c < (lim[i] & 0xFFFFu)) {
+            idx = (int)(int16_t)(lim[i] >> 16) + (int)(c >> (N - 1 - i));
+            L = (uint32_t)(16 - N + i);
+        }
+    }
+    if (idx < 0 || idx >= 288) return E_BAD;
+    const uint32_t sym = (uint32_t)sym8[idx] | (((hi8[idx >> 5] >> (idx & 31)) & 1u) << 8);
+    return sym_entry(T_LIT, sym, L);
+}
+
 __device__ __forceinline__ void report(cb_inflate_summary* summary, uint32_t* job_status, long long j, uint32_t st) {
     if (job_status) job_status[j] = st;
     if (st != CB_OK) {
@@ -243,11 +282,14 @@ __device__ __forceinline__ uint32_t load_word(const uint32_t* wbase, uint32_t nv
     return w < nvalid ? __ldg(wbase + w) : 0u;
 }
 
+// A hint to bring the 128-byte line of p into L2 (a prefetch, no load into registers).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <class C>
 __global__ void __launch_bounds__(C::WARPS * 32)
     k_decode(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
              uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes,
-             int steps) {
+             int steps, uint32_t ahead) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     typename C::CtaSmem& S = *reinterpret_cast<typename C::CtaSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -258,21 +300,27 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     long long n = n_jobs;
     if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
 
-    uint16_t* my_lit = W.lit[lane];
-    uint16_t* my_dist = W.dist[lane];
-    uint8_t* my_lens = reinterpret_cast<uint8_t*>(my_lit);  // code lengths while a header is read
+    uint8_t* const my_base = W.lane[lane];
+    const uint16_t* my_lit = reinterpret_cast<const uint16_t*>(my_base + C::LIT);
+    const uint16_t* my_dist = reinterpret_cast<const uint16_t*>(my_base + C::DIST);
+    const uint16_t* my_dsym = reinterpret_cast<const uint16_t*>(my_base + C::DSYM);
+    const uint8_t* my_lsym = my_base + C::LSYM;
+    const uint32_t* my_lhi = reinterpret_cast<const uint32_t*>(my_base + C::LHI);
+    const uint16_t* my_cltab = reinterpret_cast<const uint16_t*>(my_base);  // while a header is read
+    uint8_t* my_lens = my_base + C::LSYM;  // code lengths while a header is read (after the 19 below)
 
     // the member of this lane
     int st = S_IDLE;
     long long j = 0;
+    // bit reader: bb holds bc bits (LSB first); p0, p1 are the next two words, nw the word after them
     const uint32_t* wbase = nullptr;
-    uint32_t nvalid = 0, w = 0, lo = 0, hi = 0, off = 0;  // bit reader: lo = word w, hi = word w + 1
+    uint64_t bb = 0;
+    uint32_t bc = 0, p0 = 0, p1 = 0, nw = 0, nvalid = 0;
     uint32_t s0 = 0, in_bits = 0, isize = 0, pos = 0;
     bool final_block = false;
     uint32_t rem = 0, hlit = 0, total = 0, ci = 0;  // stored bytes left; code lengths read
-    uint64_t* slot = nullptr;
-    uint32_t nunits = 0, nq = 0, pcnt = 0;           // units written, u64 groups stored, units pending
-    uint64_t pend = 0;
+    uint32_t* slot = nullptr;
+    uint32_t nunits = 0, nwords = 0, half = 0, has = 0;  // units written, u32 words stored, a pending unit
     uint32_t err = CB_OK;
     uint32_t llim[C::NLL], dlim[C::NLD];
 #pragma unroll
@@ -280,26 +328,30 @@ __global__ void __launch_bounds__(C::WARPS * 32)
 #pragma unroll
     for (int i = 0; i < C::NLD; i++) dlim[i] = 0;
 
-    auto adv = [&](uint32_t k) {  // k <= 32
-        off += k;
-        if (off >= 32) {
-            off -= 32;
-            w++;
-            lo = hi;
-            hi = load_word(wbase, nvalid, w + 1);
+    auto refill = [&]() {  // afterwards bc >= 33
+        if (bc <= 32) {
+            bb |= (uint64_t)p0 << bc;
+            bc += 32;
+            p0 = p1;
+            p1 = load_word(wbase, nvalid, nw);
+            // entering a new 128-byte line of input: ask L2 for the line `ahead` lines further on, so
+            // that the lane's loads find its stream in L2 rather than DRAM
+            if (ahead && (nw & 31u) == 0 && nw + ahead * 32 < nvalid) prefetch_l2(wbase + nw + ahead * 32);
+            nw++;
         }
     };
-    auto window = [&]() { return __funnelshift_r(lo, hi, off); };
-    auto consumed = [&]() { return w * 32u + off - s0; };
-    auto put = [&](uint32_t v, uint32_t k) {  // append k (1 or 2) units, packed low unit first
-        const uint32_t c = pcnt;
-        pend |= (uint64_t)v << (16 * c);
-        pcnt = c + k;
-        nunits += k;
-        if (pcnt >= 4) {
-            slot[nq++] = pend;
-            pend = pcnt > 4 ? (uint64_t)(v >> 16) : 0ull;
-            pcnt -= 4;
+    auto consume = [&](uint32_t k) {  // k <= bc
+        bb >>= k;
+        bc -= k;
+    };
+    auto consumed = [&]() { return (nw - 2) * 32u - bc - s0; };  // bits of the payload used
+    auto put = [&](uint32_t v, uint32_t k) {  // append k (0, 1 or 2) units, packed low unit first
+        if (k) {
+            const uint32_t wv = has ? (half | (v << 16)) : v;
+            if (k == 2 || has) slot[nwords++] = wv;
+            half = has ? (v >> 16) : v;
+            has ^= k & 1u;
+            nunits += k;
         }
     };
     auto fail = [&](uint32_t code) {
@@ -327,18 +379,21 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                     nvalid = (uint32_t)((in + job.in_len + 8 - (uintptr_t)wbase) >> 2);
                     in_bits = job.in_len * 8u;
                     isize = job.isize;
-                    w = 0;
-                    off = s0;
-                    lo = load_word(wbase, nvalid, 0);
-                    hi = load_word(wbase, nvalid, 1);
+                    bb = 0;
+                    bc = 0;
+                    p0 = load_word(wbase, nvalid, 0);
+                    p1 = load_word(wbase, nvalid, 1);
+                    nw = 2;
+                    refill();
+                    refill();
+                    consume(s0);
                     pos = 0;
                     final_block = false;
-                    nunits = nq = pcnt = 0;
-                    pend = 0;
+                    nunits = nwords = half = has = 0;
                     err = CB_OK;
                     st = S_HDR;
                     const unsigned long long so = slot_of_job(job.out_off, j);
-                    slot = reinterpret_cast<uint64_t*>(arena + so);
+                    slot = reinterpret_cast<uint32_t*>(arena + so);
                     if (job.out_off < 0 || so + 2ull * isize + 8ull > arena_bytes) fail(CB_ERR_CAPACITY);
                     // slots are disjoint only for jobs in increasing out_off with disjoint outputs
                     else if (j + 1 < n && jobs[j + 1].out_off < job.out_off + (long long)isize) fail(CB_ERR_ARG);
@@ -352,12 +407,15 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             const int t = __ffs(b) - 1;
             const int tst = __shfl_sync(FULL, st, t);
             bool ok;
+            uint8_t* tb = W.lane[t];
             if (tst == S_BUILD_CL) {
-                // the code-length code: lengths in lane t's first 19 bytes, table into its distance table
-                const uint8_t* tl = reinterpret_cast<const uint8_t*>(W.lit[t]);
-                if (lane < 19) W.lens[lane] = tl[lane];
+                // the code-length code: its 19 lengths wait at LSYM; its table goes to the region's start,
+                // then the code lengths to come start from zero (runs of zeros are not written)
+                if (lane < 19) W.lens[lane] = tb[C::LSYM + lane];
                 __syncwarp();
-                ok = build_lane(W.lens, 19, 7, T_CL, W.dist[t], nullptr, nullptr, W.scratch);
+                ok = build_lane(W.lens, 19, 7, T_CL, reinterpret_cast<uint16_t*>(tb), nullptr, nullptr, nullptr,
+                                nullptr, W.scratch);
+                for (int k = lane; k < 80; k += 32) reinterpret_cast<uint32_t*>(tb + C::LSYM)[k] = 0;
             } else {
                 // literal/length and distance codes: fixed (hlit 0 marks a fixed block) or lane t's lengths
                 const uint32_t th = __shfl_sync(FULL, hlit, t);
@@ -369,14 +427,15 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                     nl = 288;
                     nd = 32;
                 } else {
-                    const uint8_t* tl = reinterpret_cast<const uint8_t*>(W.lit[t]);
-                    for (uint32_t s = lane; s < ttot; s += 32) W.lens[s] = tl[s];
+                    for (uint32_t s = lane; s < ttot; s += 32) W.lens[s] = tb[C::LSYM + s];
                     nl = (int)th;
                     nd = (int)(ttot - th);
                 }
                 __syncwarp();
-                ok = build_lane(W.lens, nl, C::LB, T_LIT, W.lit[t], W.lim, W.lsym[t], W.scratch) &&
-                     build_lane(W.lens + nl, nd, C::DB, T_DIST, W.dist[t], W.lim + C::NLL, W.dsym[t], W.scratch);
+                ok = build_lane(W.lens, nl, C::LB, T_LIT, reinterpret_cast<uint16_t*>(tb + C::LIT), W.lim, nullptr,
+                                tb + C::LSYM, reinterpret_cast<uint32_t*>(tb + C::LHI), W.scratch) &&
+                     build_lane(W.lens + nl, nd, C::DB, T_DIST, reinterpret_cast<uint16_t*>(tb + C::DIST),
+                                W.lim + C::NLL, reinterpret_cast<uint16_t*>(tb + C::DSYM), nullptr, nullptr, W.scratch);
             }
             __syncwarp();
             if (lane == t) {
@@ -401,17 +460,17 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             if (consumed() > in_bits) {
                 fail(CB_ERR_INFLATE);
             } else {
-                uint32_t x = window();
-                const uint32_t h = x & 7u;
-                adv(3);
+                refill();
+                const uint32_t h = (uint32_t)bb & 7u;
+                consume(3);
                 final_block = (h & 1u) != 0;
                 const uint32_t btype = h >> 1;
                 if (btype == 0) {
-                    adv((8u - (off & 7u)) & 7u);  // to a byte boundary (the payload starts on one)
-                    x = window();
+                    consume(bc & 7u);  // to a byte boundary: whole words are loaded, so bc & 7 bits remain
+                    refill();
+                    const uint32_t x = (uint32_t)bb;
                     const uint32_t len = x & 0xFFFFu, nlen = x >> 16;
-                    adv(16);
-                    adv(16);
+                    consume(32);
                     if (len != (~nlen & 0xFFFFu) || len > isize - pos || consumed() + 8ull * len > in_bits) {
                         fail(CB_ERR_INFLATE);
                     } else {
@@ -422,20 +481,22 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                     hlit = 0;  // fixed codes
                     st = S_BUILD;
                 } else if (btype == 2) {
-                    x = window();
+                    refill();
+                    const uint32_t x = (uint32_t)bb;
                     hlit = (x & 31u) + 257;
                     const uint32_t hdist = ((x >> 5) & 31u) + 1, hclen = ((x >> 10) & 15u) + 4;
-                    adv(14);
+                    consume(14);
                     if (hlit > 286 || hdist > 30) {
                         fail(CB_ERR_INFLATE);
                     } else {
                         total = hlit + hdist;
-                        uint32_t* z = reinterpret_cast<uint32_t*>(my_lens);
+                        uint32_t* zc = reinterpret_cast<uint32_t*>(my_lens);
 #pragma unroll
-                        for (int k = 0; k < 5; k++) z[k] = 0;
+                        for (int k = 0; k < 5; k++) zc[k] = 0;
                         for (uint32_t i = 0; i < hclen; i++) {
-                            my_lens[kClOrder[i]] = (uint8_t)(window() & 7u);
-                            adv(3);
+                            refill();
+                            my_lens[kClOrder[i]] = (uint8_t)(bb & 7u);
+                            consume(3);
                         }
                         st = S_BUILD_CL;
                     }
@@ -446,91 +507,86 @@ __global__ void __launch_bounds__(C::WARPS * 32)
         }
         if (st == S_FIN) {
             if (err == CB_OK && (consumed() > in_bits || pos != isize)) err = CB_ERR_INFLATE;
-            if (err == CB_OK && pcnt) slot[nq] = pend;  // the last units (the slot has 8 spare bytes)
+            if (err == CB_OK && has) slot[nwords] = half;  // the last unit (the slot has 8 spare bytes)
             per_job[2 * j] = nunits;
             per_job[2 * j + 1] = err;
             report(summary, job_status, j, err);
             st = S_IDLE;
         }
 
-        // ---- decode steps (lock step over the lanes' own streams)
+        // ---- decode steps (lock step over the lanes' own streams); one straight path per symbol
 #pragma unroll 1
         for (int k = 0; k < steps; k++) {
             if (st == S_RUN) {
-                const uint32_t x = window();
+                refill();
+                const uint32_t x = (uint32_t)bb;
                 uint32_t e = my_lit[x & C::LMASK];
-                if (e == E_LONG) e = long_entry<C::NLL, 288>(x, llim, W.lsym[lane]);
+                if (e == E_LONG) e = long_lit_entry<C::NLL>(x, llim, my_lsym, my_lhi);
                 const uint32_t L = e_len(e);
-                if (e & 0x8000u) {
-                    const uint32_t ext = (e >> 12) & 7u;
-                    const uint32_t len = (e & 255u) + 3 + ((x >> L) & ((1u << ext) - 1u));
-                    adv(L + ext);
-                    const uint32_t y = window();
-                    uint32_t d = my_dist[y & C::DMASK];
-                    if (d == E_LONG) d = long_entry<C::NLD, 32>(y, dlim, W.dsym[lane]);
-                    const uint32_t dl = e_len(d);
-                    uint32_t dbase, dext;
-                    dist_code(d & 31u, dbase, dext);
-                    const uint32_t dist = dbase + ((y >> dl) & ((1u << dext) - 1u));
-                    adv(dl + dext);
-                    if (e_kind(d) != E_DIST || (d & 0x8000u) || dist > pos || len > isize - pos) {
-                        fail(CB_ERR_INFLATE);
-                    } else {
-                        put(unit_match(len, dist), 2);
-                        pos += len;
-                    }
-                } else if (e < 0x1000u) {
-                    adv(L);
-                    if (pos >= isize) {
-                        fail(CB_ERR_INFLATE);
-                    } else {
-                        put(e & 255u, 1);
-                        pos++;
-                    }
-                } else if (e_kind(e) == E_EOB) {
-                    adv(L);
-                    st = final_block ? S_FIN : S_HDR;
-                } else {
+                const bool is_len = (e & 0x8000u) != 0;
+                const bool is_lit = e < 0x1000u;
+                const bool is_eob = !is_len && e_kind(e) == E_EOB;
+                const uint32_t ext = is_len ? (e >> 12) & 7u : 0u;
+                const uint32_t len = (e & 255u) + 3 + ((x >> L) & ((1u << ext) - 1u));
+                const uint32_t n1 = L + ext;  // <= 20 < bc
+                // the distance (used by lengths only) from the 32 bits after n1: the rest of bb and,
+                // past its bc bits, the next word -- no refill inside the step
+                const uint32_t avail = bc - n1;
+                const uint32_t y = (uint32_t)(bb >> n1) | (avail < 32 ? p0 << avail : 0u);
+                uint32_t d = my_dist[y & C::DMASK];
+                if (is_len && d == E_LONG) d = long_entry<C::NLD, 32>(y, dlim, my_dsym);
+                const uint32_t dl = e_len(d);
+                uint32_t dbase, dext;
+                dist_code(d & 31u, dbase, dext);
+                const uint32_t dist = dbase + ((y >> dl) & ((1u << dext) - 1u));
+                const uint32_t k = n1 + (is_len ? dl + dext : 0u);  // <= 48
+                if (k < bc) {
+                    consume(k);
+                } else {  // the step used bits of p0: it becomes the buffer
+                    const uint32_t r = k - bc;  // < 16
+                    bb = (uint64_t)(p0 >> r);
+                    bc = 32 - r;
+                    p0 = p1;
+                    p1 = load_word(wbase, nvalid, nw);
+                    nw++;
+                }
+                const bool bad = (!is_len && !is_lit && !is_eob) || (is_lit && pos >= isize) ||
+                                 (is_len && (e_kind(d) != E_DIST || (d & 0x8000u) || dist > pos || len > isize - pos));
+                if (bad) {
                     fail(CB_ERR_INFLATE);
+                } else {
+                    put(is_len ? unit_match(len, dist) : (e & 255u), is_len ? 2u : is_lit ? 1u : 0u);
+                    pos += is_len ? len : is_lit ? 1u : 0u;
+                    if (is_eob) st = final_block ? S_FIN : S_HDR;
                 }
             } else if (st == S_CLENS) {
-                const uint32_t x = window();
-                const uint32_t e = my_dist[x & 127u];
+                refill();
+                const uint32_t x = (uint32_t)bb;
+                const uint32_t e = my_cltab[x & 127u];
                 const uint32_t L = e_len(e), s = e & 255u;
-                if (e_kind(e) != E_CL || (e & 0x8000u) || L == 0) {
+                const uint32_t eb = s < 16 ? 0u : s == 16 ? 2u : s == 17 ? 3u : 7u;
+                const uint32_t rep = s < 16 ? 1u : (s == 18 ? 11u : 3u) + ((x >> L) & ((1u << eb) - 1u));
+                consume(L + eb);
+                if (e_kind(e) != E_CL || (e & 0x8000u) || L == 0 || (s == 16 && ci == 0) || ci + rep > total) {
                     fail(CB_ERR_INFLATE);
-                } else if (s < 16) {
-                    adv(L);
-                    my_lens[ci++] = (uint8_t)s;
                 } else {
-                    uint32_t rep, val = 0, eb;
-                    if (s == 16) {
-                        rep = 3 + ((x >> L) & 3u);
-                        eb = 2;
-                        val = ci ? my_lens[ci - 1] : 0u;
-                    } else if (s == 17) {
-                        rep = 3 + ((x >> L) & 7u);
-                        eb = 3;
-                    } else {
-                        rep = 11 + ((x >> L) & 127u);
-                        eb = 7;
+                    if (s < 16) {
+                        my_lens[ci] = (uint8_t)s;
+                    } else if (s == 16) {
+                        const uint8_t v = my_lens[ci - 1];
+                        for (uint32_t r = 0; r < rep; r++) my_lens[ci + r] = v;  // 3-6 copies
                     }
-                    adv(L + eb);
-                    if ((s == 16 && ci == 0) || ci + rep > total) {
-                        fail(CB_ERR_INFLATE);
-                    } else {
-                        for (uint32_t r = 0; r < rep; r++) my_lens[ci + r] = (uint8_t)val;
-                        ci += rep;
+                    ci += rep;
+                    if (ci == total) {
+                        if (my_lens[256] == 0) fail(CB_ERR_INFLATE);  // no end-of-block code
+                        else st = S_BUILD;
                     }
-                }
-                if (st == S_CLENS && ci == total) {
-                    if (my_lens[256] == 0) fail(CB_ERR_INFLATE);  // no end-of-block code
-                    else st = S_BUILD;
                 }
             } else if (st == S_STORED) {
-                const uint32_t x = window();
+                refill();
+                const uint32_t x = (uint32_t)bb;
                 const uint32_t k2 = rem >= 2 ? 2u : 1u;
-                adv(8 * k2);
+                consume(8 * k2);
                 put(k2 == 2 ? ((x & 255u) | ((x << 8) & 0xFF0000u)) : (x & 255u), k2);
                 pos += k2;
                 rem -= k2;
@@ -542,18 +598,25 @@ __global__ void __launch_bounds__(C::WARPS * 32)
 
 // ---------------------------------------------------------------- k_copy: one member per warp
 
-constexpr uint32_t RING = 32768;          // every DEFLATE distance reads the ring
-constexpr uint32_t RMASK = RING - 1;
 constexpr int WIN = 1024;                 // flush and CRC window
 static_assert(WIN == 32 * 32, "one 32-byte CRC column per lane");
 
-template <int WARPS_>
+// WARPS_ warps per CTA, each with a ring of RING_ bytes: sources up to RING_ - 32 bytes back read
+// the ring, older ones the output already stored in HBM.
+template <int WARPS_, uint32_t RING_>
 struct CopyCfg {
     static constexpr int WARPS = WARPS_;
+    static constexpr uint32_t RING = RING_, RMASK = RING_ - 1;
+    // a group's tokens start within GMAX bytes: its output (GMAX + 258 at most) and the unflushed
+    // window before it (under WIN bytes) stay in the ring while the group is written
+    static constexpr uint32_t GMAX = RING_ - WIN - 258 - 64;
+    static_assert((RING_ & (RING_ - 1)) == 0 && RING_ >= 4096, "ring size");
     struct CtaSmem {
         uint32_t crc8[8][256];
         uint32_t mulk[4][256];   // x * x^(8 (WIN - 32)) by bytes: moves a column past the other lanes
-        alignas(16) uint8_t ring[WARPS_][RING];
+        uint32_t tok[WARPS_][32];  // the tokens of the warp's current group, in order
+        uint32_t tokq[WARPS_][32]; // their start within the group | length << 16
+        alignas(16) uint8_t ring[WARPS_][RING_];
     };
 };
 
@@ -565,7 +628,7 @@ __device__ __forceinline__ uint32_t mulk(const S& s, uint32_t x) {
 // Store output bytes [ws, we) from the ring (byte p at slot p + a) to out, and fold them into this
 // lane's CRC column (window kwin; windows are aligned to the end of the member, the first one
 // padded by `pad` zero bytes in front).
-template <class S>
+template <uint32_t RMASK, class S>
 __device__ __noinline__ uint32_t flush_window(uint8_t* out, uint32_t a, uint32_t ws, uint32_t we, uint32_t kwin,
                                               uint32_t pad, uint32_t col, const uint8_t* ring, const S& s, bool crc) {
     const int lane = threadIdx.x & 31;
@@ -586,19 +649,31 @@ __device__ __noinline__ uint32_t flush_window(uint8_t* out, uint32_t a, uint32_t
     if (crc) {
         uint32_t c = mulk(s, col);
         const long long v0 = (long long)kwin * WIN + 32 * lane - (long long)pad;  // position of the column
+        uint32_t wv[8];
+        if (v0 >= 0) {
+            // the column's 32 bytes from 9 aligned ring words (funnel shifts for the byte phase)
+            const uint32_t sl = (uint32_t)(v0 + a) & RMASK, w = sl >> 2, sh = (sl & 3u) * 8;
+            const uint32_t* rw = reinterpret_cast<const uint32_t*>(ring);
+            uint32_t r[9];
 #pragma unroll
-        for (int q = 0; q < 32; q += 8) {
-            uint32_t w0 = 0, w1 = 0;
+            for (int k = 0; k < 9; k++) r[k] = rw[(w + k) & (RMASK >> 2)];
 #pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const long long r0 = v0 + q + t, r1 = v0 + q + 4 + t;
-                const uint32_t b0 = r0 >= 0 ? ring[(uint32_t)(r0 + a) & RMASK] : 0u;
-                const uint32_t b1 = r1 >= 0 ? ring[(uint32_t)(r1 + a) & RMASK] : 0u;
-                w0 |= b0 << (8 * t);
-                w1 |= b1 << (8 * t);
+            for (int k = 0; k < 8; k++) wv[k] = __funnelshift_r(r[k], r[k + 1], sh);
+        } else {
+            // the first window: zero bytes stand before the member's start
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                uint32_t v = 0;
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    const long long r0 = v0 + 4 * k + t;
+                    v |= (r0 >= 0 ? (uint32_t)ring[(uint32_t)(r0 + a) & RMASK] : 0u) << (8 * t);
+                }
+                wv[k] = v;
             }
-            c = crc_step8(s.crc8, c, w0, w1);
         }
+#pragma unroll
+        for (int q = 0; q < 8; q += 2) c = crc_step8(s.crc8, c, wv[q], wv[q + 1]);
         col = c;
     }
     __syncwarp();
@@ -633,6 +708,9 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint8_t* ring = S.ring[warp];
+    uint32_t* tokw = S.tok[warp];
+    uint32_t* tokq = S.tokq[warp];
+    const uint32_t incl = lane == 31 ? 0xFFFFFFFFu : (2u << lane) - 1u;  // lanes 0..lane
     unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + 1;
     const uint32_t* per_job = reinterpret_cast<const uint32_t*>(ws + WS_HEAD);
     const uint8_t* arena = ws + arena_offset(n_jobs);
@@ -662,43 +740,69 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             const uint32_t avail = min(32u, nu - g);
             const uint32_t nxt = __shfl_down_sync(FULL, u, 1);
             const bool head31 = avail == 32 && (__shfl_sync(FULL, u, 31) & 0xC000u) == 0x8000u;
-            const uint32_t cnt = avail - (head31 ? 1u : 0u);
+            uint32_t cnt = avail - (head31 ? 1u : 0u);
+            const bool unit_head = (u & 0xC000u) == 0x8000u, unit_tail = (u & 0xC000u) == 0xC000u;
+            uint32_t len = (uint32_t)lane < cnt ? (!(u & 0x8000u) ? 1u : unit_head ? ((u >> 6) & 255u) + 3 : 0u) : 0u;
+            uint32_t glen;
+            uint32_t ex = warp_exclusive_scan(len, glen);
+            if (glen > C::GMAX) {
+                // keep the units whose token starts within GMAX bytes (a tail goes with its head)
+                const uint32_t ex_prev = __shfl_up_sync(FULL, ex, 1);
+                const uint32_t start = (unit_tail && lane > 0) ? ex_prev : ex;
+                cnt = __popc(__ballot_sync(FULL, (uint32_t)lane < cnt && start < C::GMAX));
+                if ((uint32_t)lane >= cnt) len = 0;
+                ex = warp_exclusive_scan(len, glen);
+            }
             const bool valid = (uint32_t)lane < cnt;
-            const bool is_lit = valid && !(u & 0x8000u);
-            const bool is_head = valid && (u & 0xC000u) == 0x8000u;
+            const bool is_head = valid && unit_head;
             // a head's tail is the next unit of the group (a head at the end of the units is an error)
             const bool bad_head = is_head && ((uint32_t)lane + 1 >= cnt || (nxt & 0xC000u) != 0xC000u);
-            const uint32_t len = is_lit ? 1u : is_head ? ((u >> 6) & 255u) + 3 : 0u;
             const uint32_t dist = is_head ? ((((u & 63u) << 9) | (nxt & 511u)) + 1) : 0u;
             // the next group's units are loaded while this one is written
             const uint32_t g2 = g + cnt;
             const uint32_t u2 = (g2 + lane < nu) ? (uint32_t)__ldcs(U + g2 + lane) : 0u;
-            uint32_t glen;
-            const uint32_t ex = warp_exclusive_scan(len, glen);
             if (__any_sync(FULL, bad_head || (is_head && dist > p + ex)) || glen > isize - p) {
                 st = CB_ERR_INFLATE;
                 break;
             }
-            // token word: literal byte, or 0x80000000 | distance
-            const uint32_t tw = is_head ? (0x80000000u | dist) : (u & 255u);
+            // the group's tokens in order (tails are not tokens): literal byte, or 0x80000000 | distance
+            const bool is_tok = len != 0;
+            const unsigned tokmask = __ballot_sync(FULL, is_tok);
+            if (is_tok) {
+                const uint32_t o = __popc(tokmask & ((1u << lane) - 1u));
+                tokw[o] = is_head ? (0x80000000u | dist) : (u & 255u);
+                tokq[o] = ex | (len << 16);
+            }
+            __syncwarp();
+            uint32_t before = 0;  // tokens that start before this round
             for (uint32_t r0 = 0; r0 < glen; r0 += 32) {
                 const uint32_t rel = r0 + lane;
-                // the token of byte rel: the last lane with ex <= rel (tails carry the next token's ex)
-                int k = 0;
-#pragma unroll
-                for (int step = 16; step; step >>= 1) {
-                    const int c = k + step;
-                    const uint32_t exc = __shfl_sync(FULL, ex, c & 31);
-                    if ((uint32_t)c < cnt && exc <= rel) k = c;
-                }
-                const uint32_t t = __shfl_sync(FULL, tw, k);
+                // the token of byte rel: tokens starting in this round set bits of a mask; the byte's
+                // token is the last one starting at or before it
+                const uint32_t sm = __reduce_or_sync(FULL, (is_tok && ex >= r0 && ex < r0 + 32) ? 1u << (ex - r0) : 0u);
+                const uint32_t ord = before + __popc(sm & incl) - 1;
+                before += __popc(sm);
+                const uint32_t t = tokw[ord & 31u];
                 const uint32_t b = p + rel;
                 uint32_t val = t & 255u;
                 int src = lane;  // the lane of this round holding the byte's source
                 if (rel < glen && (t & 0x80000000u)) {
-                    const uint32_t x = b - (t & 0x7FFFFFFFu);
+                    const uint32_t d = t & 0x7FFFFFFFu;
+                    uint32_t x = b - d;
+                    const uint32_t tq = tokq[ord & 31u], q = p + (tq & 0xFFFFu);
+                    if (x >= q) {
+                        // an overlapping match repeats the d bytes before it: take the byte one period
+                        // back from the token's start, x = q - d + (b - q) mod d
+                        const uint32_t m = b - q;
+                        uint32_t k = (uint32_t)((float)m * __frcp_rn((float)d));
+                        int r = (int)m - (int)(k * d);
+                        if (r < 0) r += (int)d;
+                        if (r >= (int)d) r -= (int)d;
+                        x = q - d + (uint32_t)r;
+                    }
                     if (x >= p + r0) src = (int)(x - (p + r0));
-                    else val = ring[(x + a) & RMASK];
+                    else if (x + C::RING >= p + r0 + 32) val = ring[(x + a) & C::RMASK];
+                    else val = __ldcg(out + x);  // flushed long ago (the ring keeps the last RING - 32 bytes)
                 }
                 bool need = src != lane;
                 for (int it = 0; it < 6 && __any_sync(FULL, need); it++) {
@@ -714,12 +818,13 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                         }
                     }
                 }
-                if (rel < glen) ring[(b + a) & RMASK] = (uint8_t)val;
+                if (rel < glen) ring[(b + a) & C::RMASK] = (uint8_t)val;
                 __syncwarp();
             }
+            __syncwarp();  // the round loop read tokw; the next group writes it
             p += glen;
             while (we > ws_ && p >= we) {
-                col = flush_window(out, a, ws_, we, kwin, pad, col, ring, S, crc);
+                col = flush_window<C::RMASK>(out, a, ws_, we, kwin, pad, col, ring, S, crc);
                 ws_ = we;
                 we = min(we + WIN, isize);
                 kwin++;
@@ -786,7 +891,8 @@ int launch_decode(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_
     const long long by_work = (n_jobs + 32 * D::WARPS - 1) / (32 * D::WARPS);
     if (!d_n_jobs && by_work < grid) grid = by_work;
     split::k_decode<D><<<(unsigned)(grid < 1 ? 1 : grid), D::WARPS * 32, smem, s>>>(
-        jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, (int)cb_param(CB_PARAM_DECODE_STEPS));
+        jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, (int)cb_param(CB_PARAM_DECODE_STEPS),
+        (uint32_t)cb_param(CB_PARAM_DECODE_PREFETCH));
     return CB_OK;
 }
 
@@ -822,18 +928,30 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
     split::k_split_init<<<1, 1, 0, s>>>(summary, reinterpret_cast<unsigned long long*>(ws));
     if (n_jobs > 0) {
         const int rb = (int)cb_param(CB_PARAM_DECODE_ROOT);
-        int rc = rb == 9 ? launch_decode<split::DecCfg<9, 7, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws,
-                                                                 arena_bytes, s)
-                         : launch_decode<split::DecCfg<8, 7, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws,
-                                                                 arena_bytes, s);
+        int rc;
+        if (rb == 8)
+            rc = launch_decode<split::DecCfg<8, 6, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
+        else if (rb == 7)
+            rc = launch_decode<split::DecCfg<7, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
+        else
+            rc = launch_decode<split::DecCfg<6, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
         if (rc != CB_OK) return rc;
         const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
         if (cw == 2)
-            rc = launch_copy<split::CopyCfg<2>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
-        else if (cw == 6)
-            rc = launch_copy<split::CopyCfg<6>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
+            rc = launch_copy<split::CopyCfg<2, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
+                                                      ws, s);
+        else if (cw == 3)
+            rc = launch_copy<split::CopyCfg<3, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
+                                                      ws, s);
+        else if (cw == 12)
+            rc = launch_copy<split::CopyCfg<12, 8192>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
+                                                      ws, s);
+        else if (cw == 24)
+            rc = launch_copy<split::CopyCfg<24, 4096>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
+                                                      ws, s);
         else
-            rc = launch_copy<split::CopyCfg<3>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s);
+            rc = launch_copy<split::CopyCfg<6, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
+                                                      ws, s);
         if (rc != CB_OK) return rc;
     }
     split::k_split_finish<<<1, 1, 0, s>>>(summary);

@@ -90,17 +90,21 @@ int cb_device_sm_count(void);
  * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
  *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB (32 KiB)
  *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (1)
- *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 8 or 9 (8)
- *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 (3)
+ *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 6, 7 or 8 (7)
+ *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 with a 16 KiB window per
+ *                          warp, 12 with an 8 KiB window, 24 with a 4 KiB window (12)
  *   CB_PARAM_DECODE_STEPS  decode steps of form 3 between lane scheduling rounds: 1-64 (16)
- * cb_set_param(key, 0) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
+ *   CB_PARAM_DECODE_PREFETCH  lines (128 B) of compressed input form 3's decoder asks L2 for ahead of
+ *                          each lane's position: 0-16, 0 = none (4)
+ * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
     CB_PARAM_CHAIN_TILE = 1,
     CB_PARAM_INFLATE_FORM = 2,
     CB_PARAM_DECODE_ROOT = 3,
     CB_PARAM_COPY_WARPS = 4,
-    CB_PARAM_DECODE_STEPS = 5
+    CB_PARAM_DECODE_STEPS = 5,
+    CB_PARAM_DECODE_PREFETCH = 6
 };
 int cb_set_param(int key, int64_t value);
 int64_t cb_get_param(int key);
