@@ -354,7 +354,10 @@ def run_ours(args):
     value = whole_job(inflated, ms, world) / 1e9
     peak, peak_kind = peaks()
     achieved = inflated / (inflate_ms / 1e3) / 1e9
-    kernel = "k_inflate_warp"  # the form cb_inflate runs
+    from cubam_b200.bgzf import inflate_form
+
+    form = inflate_form(0)  # the form the batched decode runs
+    kernel = {1: "k_inflate_warp", 2: "k_inflate_lanes", 3: "k_decode + k_copy"}[form]
 
     # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)
     plain = None
@@ -409,6 +412,7 @@ def run_ours(args):
         "roofline": {
             "bound": "hbm",
             "kernel": kernel,
+            "form": form,
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -639,7 +643,7 @@ def run_uneven(args):
     ms_per_file = s2.elapsed_time(e2)
     peak, peak_kind = peaks()
     achieved = inflated / (stage["inflated"] / 1e3) / 1e9
-    kernel = "k_inflate_lanes" if plan.form == 2 else "k_inflate_warp"
+    kernel = {1: "k_inflate_warp", 2: "k_inflate_lanes", 3: "k_decode + k_copy"}[plan.form]
     print(json.dumps({
         "metric": METRIC, "value": inflated / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

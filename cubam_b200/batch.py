@@ -27,10 +27,24 @@ import torch
 
 from cubam_b200 import _lib
 from cubam_b200.bam import _TYPES, FIELDS, BamHeader, Tag
-from cubam_b200.bgzf import ctypes_sizeof, raise_status, read_struct, stream_ptr
+from cubam_b200.bgzf import (
+    ctypes_sizeof,
+    inflate_form,
+    inflate_workspace_bytes,
+    launch_inflate,
+    raise_status,
+    read_struct,
+    stream_ptr,
+)
 
 #: kernels launched by each entry point (for the launch count of a step)
 KERNELS = {"scan": 4, "inflate": 3, "chain": 5, "decode": 1, "tags": 1}
+
+
+def inflate_launches(form: int = 0) -> int:
+    """Kernels of one inflate call: init, the persistent grid, finish; form 3 adds the slot scan and
+    splits the grid into decode and copy."""
+    return 5 if inflate_form(form) == 3 else KERNELS["inflate"]
 
 
 @dataclass
@@ -139,13 +153,12 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
     if events:
         events.mark("scanned")
     inflate_summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device="cuda")
-    qws = torch.empty(256, dtype=torch.uint8, device="cuda")
     if n_jobs:
-        rc = _lib.lib.cb_inflate(all_jobs.data_ptr(), n_jobs, None, out.data_ptr(), int(check_crc), None,
-                                 inflate_summ.data_ptr(), qws.data_ptr(), qws.numel(), stream_ptr())
-        _lib.check(rc, "cb_inflate")
+        qws = torch.empty(inflate_workspace_bytes(n_jobs, total), dtype=torch.uint8, device="cuda")
+        launch_inflate(all_jobs.data_ptr(), n_jobs, out.data_ptr(), total, check_crc, inflate_summ.data_ptr(), qws)
+        del qws
         if counter is not None:
-            counter["launches"] = counter.get("launches", 0) + KERNELS["inflate"]
+            counter["launches"] = counter.get("launches", 0) + inflate_launches()
     if events:
         events.mark("inflated")
     chains = []
@@ -286,8 +299,7 @@ class BatchPlan:
         self.jobs = torch.empty(max(self.job_base[-1], 1) * _lib.JOB_BYTES, dtype=torch.uint8, device=dev)
         self.out = torch.empty(max(self.total_out, 1), dtype=torch.uint8, device=dev)
         self.inflate_summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device=dev)
-        self.queue_ws = torch.empty(max(int(_lib.lib.cb_inflate_workspace_bytes()), 256), dtype=torch.uint8,
-                                    device=dev)
+        self.queue_ws = None  # sized for the form (autotune or launch)
         self.data = []
         for (comp, header), b, total in zip(files, self.out_base, self.inflated):
             self.data.append(self.out[b + header.size : b + total])
@@ -336,10 +348,14 @@ class BatchPlan:
             _lib.check(rc, "cb_scan_members")
         if events:
             events.mark("scanned")
-        rc = _lib.lib.cb_inflate_form(self.jobs.data_ptr(), self.job_base[-1], None, self.out.data_ptr(),
-                                      int(self.check_crc), None, self.inflate_summ.data_ptr(),
-                                      self.queue_ws.data_ptr(), self.queue_ws.numel(), int(form), s)
-        _lib.check(rc, "cb_inflate_form")
+        need = inflate_workspace_bytes(self.job_base[-1], self.total_out, form)
+        if self.queue_ws is None or self.queue_ws.numel() < need:
+            if self.graph is not None:
+                raise RuntimeError("the captured plan's inflate workspace is too small for this form")
+            self.queue_ws = torch.empty(max(need, 512), dtype=torch.uint8, device="cuda")
+        ws = self.queue_ws if inflate_form(form) == 3 else self.queue_ws[: int(_lib.lib.cb_inflate_workspace_bytes())]
+        launch_inflate(self.jobs.data_ptr(), self.job_base[-1], self.out.data_ptr(), self.total_out, self.check_crc,
+                       self.inflate_summ.data_ptr(), ws, form)
         if events:
             events.mark("inflated")
         for k, ((comp, header), data, off, nrec) in enumerate(zip(self.files, self.data, self.offsets,
@@ -371,7 +387,7 @@ class BatchPlan:
         """Kernels of this library in one :meth:`launch` (the graph holds the same)."""
         chains = sum(1 for d in self.data if int(d.numel()))
         decodes = sum(1 for n in self.n_records if n)
-        return (KERNELS["scan"] * self.n_files + KERNELS["inflate"] + KERNELS["chain"] * chains
+        return (KERNELS["scan"] * self.n_files + inflate_launches(self.form or 0) + KERNELS["chain"] * chains
                 + (KERNELS["decode"] + (KERNELS["tags"] if self.tags else 0)) * decodes)
 
     def check(self) -> None:
@@ -392,10 +408,10 @@ class BatchPlan:
 
     # ------------------------------------------------------------------ tuning and graphs
     def autotune(self, reps: int = 2) -> dict:
-        """Time the batch with each inflate form (members per CTA: 8 one per warp, 128 one per lane) and
-        keep the faster; returns the inflate milliseconds per form."""
+        """Time the batch with each inflate form (1: a member per warp, 2: a member per lane, 3: decode per
+        lane and copy per warp) and keep the fastest; returns the inflate milliseconds per form."""
         times = {}
-        for form in (1, 2):
+        for form in (1, 2, 3):
             self.launch(form)
             torch.cuda.synchronize()
             self.check()

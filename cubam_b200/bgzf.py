@@ -12,8 +12,9 @@ Same API and chunk semantics as cubam's ``src/cubam/bgzf.py`` read side
    every BGZF header, the chain from offset 0 is kept and checked, and one
    inflate job per non-empty member is written with its output offset.  The
    compressed bytes of the incomplete last member stay on the GPU.
-3. **Inflate.** ``cb_inflate``: one warp per member, persistent grid, with the
-   CRC32 and ISIZE checks.
+3. **Inflate.** ``cb_inflate_form`` in the library's default form (form 3:
+   the Huffman decode with one member per lane into a token arena, then the
+   copy with one member per warp), with the CRC32 and ISIZE checks.
 
 Errors are the reference's ``ValueError`` messages; a CRC32 mismatch (which
 cubam does not check) is a ``ValueError`` too, unless ``check_crc=False``.
@@ -219,31 +220,40 @@ def scan_members(buf: torch.Tensor, eof: bool, out_base: int = 0, jobs_cap: int 
         return jobs, s
 
 
+def inflate_form(form: int = 0) -> int:
+    """The inflate form a call with ``form`` runs: 0 is the library's default (``CB_PARAM_INFLATE_FORM``)."""
+    return int(_lib.lib.cb_get_param(_lib.PARAM_INFLATE_FORM)) if form == 0 else int(form)
+
+
+def inflate_workspace_bytes(n_jobs: int, out_bytes: int, form: int = 0) -> int:
+    """Workspace bytes of an inflate of ``n_jobs`` jobs writing ``out_bytes`` bytes in total, in ``form``."""
+    if inflate_form(form) == 3:
+        return max(int(_lib.lib.cb_inflate_split_workspace_bytes(n_jobs, out_bytes)), 512)
+    return int(_lib.lib.cb_inflate_workspace_bytes())
+
+
+def launch_inflate(jobs_ptr: int, n_jobs: int, out_ptr, out_bytes: int, check_crc: bool, summary_ptr: int,
+                   workspace: torch.Tensor, form: int = 0, job_status_ptr=None, d_n_jobs_ptr=None) -> None:
+    """``cb_inflate_form`` on the current stream with a workspace from :func:`inflate_workspace_bytes`
+    (a workspace larger than the forms-1/2 size selects form 3 when the form asks for it)."""
+    rc = _lib.lib.cb_inflate_form(jobs_ptr, n_jobs, d_n_jobs_ptr, out_ptr, int(check_crc), job_status_ptr, summary_ptr,
+                                  workspace.data_ptr(), workspace.numel(), inflate_form(form), stream_ptr())
+    _lib.check(rc, "cb_inflate_form")
+
+
 def inflate_jobs(jobs: torch.Tensor, n_jobs: int, out: torch.Tensor, check_crc: bool = True, form: int = 0,
                  job_status: torch.Tensor | None = None) -> torch.Tensor:
     """Launch ``cb_inflate_form`` of ``n_jobs`` jobs into ``out``; returns the device summary (no sync).
 
-    ``form`` 0 lets the library choose (as ``cb_inflate``), 1 is one member per warp, 2 one per lane,
-    3 the two-kernel form (``cb_inflate_split``: decode one member per lane, copy one per warp).
+    ``form`` 0 lets the library choose (``CB_PARAM_INFLATE_FORM``), 1 is one member per warp, 2 one per
+    lane, 3 the two-kernel form (``cb_inflate_split``: decode one member per lane, copy one per warp).
     ``job_status`` (device uint32/int32 of ``n_jobs``) receives a status code per job when given.
     """
     summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device="cuda")
-    if form == 3:
-        ws = _workspace(_lib.lib.cb_inflate_split_workspace_bytes(n_jobs, int(out.numel())))
-        rc = _lib.lib.cb_inflate_split(
-            jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc),
-            job_status.data_ptr() if job_status is not None else None,
-            summ.data_ptr(), ws.data_ptr(), ws.numel(), stream_ptr(),
-        )
-        _lib.check(rc, "cb_inflate_split")
-        return summ
-    ws = _workspace(_lib.lib.cb_inflate_workspace_bytes())
-    rc = _lib.lib.cb_inflate_form(
-        jobs.data_ptr(), n_jobs, None, out.data_ptr() if out.numel() else None, int(check_crc),
-        job_status.data_ptr() if job_status is not None else None,
-        summ.data_ptr(), ws.data_ptr(), ws.numel(), int(form), stream_ptr(),
-    )
-    _lib.check(rc, "cb_inflate_form")
+    out_bytes = int(out.numel())
+    ws = _workspace(inflate_workspace_bytes(n_jobs, out_bytes, form))
+    launch_inflate(jobs.data_ptr(), n_jobs, out.data_ptr() if out_bytes else None, out_bytes, check_crc,
+                   summ.data_ptr(), ws, form, job_status.data_ptr() if job_status is not None else None)
     return summ
 
 

@@ -31,7 +31,7 @@ struct Param {
 };
 constexpr Param kParams[] = {
     {CB_PARAM_CHAIN_TILE, 2048, 1 << 22, 32768},
-    {CB_PARAM_INFLATE_FORM, 1, 3, 1},
+    {CB_PARAM_INFLATE_FORM, 1, 3, 3},
     {CB_PARAM_DECODE_ROOT, 6, 8, 7},
     {CB_PARAM_COPY_WARPS, 2, 24, 12},
     {CB_PARAM_DECODE_STEPS, 1, 64, 16},

@@ -29,9 +29,7 @@
 //     the CRC32 (32 lane columns joined in GF(2)).
 //
 // Units are at most one per output byte, so a member's units take at most 2 ISIZE bytes: the arena
-// holds member i at an 8-byte aligned slot from 2 out_off + 16 i (jobs in increasing out_off with
-// disjoint outputs, as the member scan writes them; a job out of that order is a CB_ERR_ARG of its
-// own).
+// gives every member a slot of 2 ISIZE + 8 bytes at the prefix sum of the slots before it.
 //
 // Every loop is bounded: each decode step consumes input bits or produces output bytes, both
 // bounded per member; every shared-memory index is masked or checked; arena and output writes
@@ -108,15 +106,38 @@ __device__ __forceinline__ uint32_t unit_match(uint32_t len, uint32_t dist) {
     return (0x8000u | ((len - 3) << 6) | (d >> 9)) | ((0xC000u | (d & 0x1FFu)) << 16);
 }
 
-// Workspace: [0, 256) queue counters; per job (units, status) as two u32; the arena after that,
-// 256-byte aligned.
+// Workspace: [0, 256) queue counters; per job 16 bytes (units u32, status u32, arena slot u64); the
+// arena after that, 256-byte aligned.  Job j's slot is the prefix sum of 2 ISIZE + 8 over the jobs
+// before it (k_slots), so the arena holds 2 sum(ISIZE) + 8 n_jobs bytes whatever the jobs' output
+// offsets are.
 constexpr size_t WS_HEAD = 256;
+constexpr size_t PER_JOB = 16;
 __host__ __device__ __forceinline__ size_t arena_offset(long long n_jobs) {
-    return (WS_HEAD + 8 * (size_t)n_jobs + 255) & ~(size_t)255;
+    return (WS_HEAD + PER_JOB * (size_t)n_jobs + 255) & ~(size_t)255;
 }
-// Byte offset of job j's slot in the arena (8-byte aligned; 2 ISIZE + 8 bytes long).
-__device__ __forceinline__ unsigned long long slot_of_job(long long out_off, long long j) {
-    return ((unsigned long long)(2 * out_off + 16 * j) + 7ull) & ~7ull;
+__host__ __device__ __forceinline__ unsigned long long slot_bytes(uint32_t isize) {
+    return 2ull * isize + 8ull;
+}
+
+// The arena slot of every job: one CTA; thread t sums a contiguous run of jobs, a block scan joins
+// the runs, and each thread writes its run's offsets.
+constexpr int SLOT_NT = 1024;
+__global__ void __launch_bounds__(SLOT_NT) k_slots(const cb_member_job* __restrict__ jobs, int64_t n_jobs,
+                                                   const int64_t* __restrict__ d_n_jobs, uint8_t* ws) {
+    __shared__ unsigned long long sm[33];
+    long long n = n_jobs;
+    if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
+    const long long per = (n + SLOT_NT - 1) / SLOT_NT;
+    const long long a = min((long long)threadIdx.x * per, n), b = min(a + per, n);
+    unsigned long long sum = 0;
+    for (long long j = a; j < b; j++) sum += slot_bytes(jobs[j].isize);
+    unsigned long long total;
+    unsigned long long off = block_exclusive_scan<SLOT_NT>(sum, total, sm);
+    unsigned long long* slot = reinterpret_cast<unsigned long long*>(ws + WS_HEAD);
+    for (long long j = a; j < b; j++) {
+        slot[2 * j + 1] = off;
+        off += slot_bytes(jobs[j].isize);
+    }
 }
 
 // ---------------------------------------------------------------- k_decode: one member per lane
@@ -295,7 +316,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     typename C::WarpSmem& W = S.w[warp];
     unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws);
-    uint32_t* per_job = reinterpret_cast<uint32_t*>(ws + WS_HEAD);  // (units, status) per job
+    uint32_t* per_job = reinterpret_cast<uint32_t*>(ws + WS_HEAD);  // (units, status, slot lo, slot hi) per job
     uint8_t* arena = ws + arena_offset(n_jobs);
     long long n = n_jobs;
     if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
@@ -392,11 +413,9 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                     nunits = nwords = half = has = 0;
                     err = CB_OK;
                     st = S_HDR;
-                    const unsigned long long so = slot_of_job(job.out_off, j);
+                    const unsigned long long so = reinterpret_cast<const unsigned long long*>(per_job)[2 * j + 1];
                     slot = reinterpret_cast<uint32_t*>(arena + so);
-                    if (job.out_off < 0 || so + 2ull * isize + 8ull > arena_bytes) fail(CB_ERR_CAPACITY);
-                    // slots are disjoint only for jobs in increasing out_off with disjoint outputs
-                    else if (j + 1 < n && jobs[j + 1].out_off < job.out_off + (long long)isize) fail(CB_ERR_ARG);
+                    if (so + slot_bytes(isize) > arena_bytes) fail(CB_ERR_CAPACITY);
                 }
             }
         }
@@ -508,8 +527,8 @@ __global__ void __launch_bounds__(C::WARPS * 32)
         if (st == S_FIN) {
             if (err == CB_OK && (consumed() > in_bits || pos != isize)) err = CB_ERR_INFLATE;
             if (err == CB_OK && has) slot[nwords] = half;  // the last unit (the slot has 8 spare bytes)
-            per_job[2 * j] = nunits;
-            per_job[2 * j + 1] = err;
+            per_job[4 * j] = nunits;
+            per_job[4 * j + 1] = err;
             report(summary, job_status, j, err);
             st = S_IDLE;
         }
@@ -723,10 +742,11 @@ __global__ void __launch_bounds__(C::WARPS * 32)
         if (lane == 0) jj = atomicAdd(queue, 1ull);
         const long long j = (long long)__shfl_sync(FULL, jj, 0);
         if (j >= n) break;
-        if (per_job[2 * j + 1] != CB_OK) continue;  // k_decode reported it
+        if (per_job[4 * j + 1] != CB_OK) continue;  // k_decode reported it
         const cb_member_job job = jobs[j];
-        const uint32_t nu = per_job[2 * j];
-        const uint16_t* U = reinterpret_cast<const uint16_t*>(arena + slot_of_job(job.out_off, j));
+        const uint32_t nu = per_job[4 * j];
+        const uint16_t* U =
+            reinterpret_cast<const uint16_t*>(arena + reinterpret_cast<const unsigned long long*>(per_job)[2 * j + 1]);
         uint8_t* out = out_base + job.out_off;
         const uint32_t a = (uint32_t)((uintptr_t)out & 15);
         const uint32_t isize = job.isize;
@@ -915,7 +935,7 @@ int launch_copy(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jo
 
 extern "C" size_t cb_inflate_split_workspace_bytes(int64_t n_jobs, int64_t out_bytes) {
     if (n_jobs < 0 || out_bytes < 0) return 0;
-    return split::arena_offset(n_jobs) + 2 * (size_t)out_bytes + 16 * (size_t)n_jobs + 16;
+    return split::arena_offset(n_jobs) + 2 * (size_t)out_bytes + 8 * (size_t)n_jobs + 16;
 }
 
 extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
@@ -927,6 +947,7 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
     const unsigned long long arena_bytes = workspace_bytes - split::arena_offset(n_jobs);
     split::k_split_init<<<1, 1, 0, s>>>(summary, reinterpret_cast<unsigned long long*>(ws));
     if (n_jobs > 0) {
+        split::k_slots<<<1, split::SLOT_NT, 0, s>>>(jobs, n_jobs, d_n_jobs, ws);
         const int rb = (int)cb_param(CB_PARAM_DECODE_ROOT);
         int rc;
         if (rb == 8)

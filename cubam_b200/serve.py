@@ -39,7 +39,15 @@ import torch
 from cubam_b200 import _lib
 from cubam_b200.bam import _TYPES, FIELDS, BamHeader, Tag
 from cubam_b200.batch import DecodedFile, _View, decode_many
-from cubam_b200.bgzf import ctypes_sizeof, raise_status, read_struct, scan_members, stream_ptr
+from cubam_b200.bgzf import (
+    ctypes_sizeof,
+    inflate_workspace_bytes,
+    launch_inflate,
+    raise_status,
+    read_struct,
+    scan_members,
+    stream_ptr,
+)
 
 #: device bytes per record besides the inflated bytes: offset, 11 columns, 21 bytes per tag
 RECORD_BYTES = 8 + 43
@@ -294,10 +302,9 @@ def decode_alone(rf: ResidentFile, req: Request, tags=("CB", "UB", "GN"), check_
     if req._region_size:
         rows = _job_rows(rf, req.m0, last, 0, req.m0)
         jobs = torch.from_numpy(rows).cuda()
-        qws = torch.empty(256, dtype=torch.uint8, device="cuda")
-        rc = _lib.lib.cb_inflate(jobs.data_ptr(), len(rows), None, region.data_ptr(), int(check_crc), None,
-                                 summ.data_ptr(), qws.data_ptr(), qws.numel(), s)
-        _lib.check(rc, "cb_inflate")
+        qws = torch.empty(inflate_workspace_bytes(len(rows), req._region_size), dtype=torch.uint8, device="cuda")
+        launch_inflate(jobs.data_ptr(), len(rows), region.data_ptr(), req._region_size, check_crc, summ.data_ptr(),
+                       qws)
     start = int(ix.first_rec[req.m0])
     data = region[start : start + req.inflated_bytes]
     off = torch.empty(max(req.n_records, 1), dtype=torch.int64, device="cuda")
@@ -449,10 +456,10 @@ class Server:
             host = torch.from_numpy(np.concatenate(rows)).pin_memory()
             jobs = scratch.get("jobs", host.numel() * 8)
             jobs[: host.numel() * 8].view(torch.int64).copy_(host.view(-1), non_blocking=True)
-            qws = scratch.get("queue", 256)
-            rc = _lib.lib.cb_inflate(jobs.data_ptr(), n_jobs, None, self.pool.data_ptr(), int(self.check_crc), None,
-                                     summ.data_ptr(), qws.data_ptr(), qws.numel(), s)
-            _lib.check(rc, "cb_inflate")
+            out_bytes = int(sum(int((x[:, 2] >> 32).sum()) for x in rows))  # sum of ISIZE (high half of word 2)
+            qws = scratch.get("queue", inflate_workspace_bytes(n_jobs, out_bytes))
+            launch_inflate(jobs.data_ptr(), n_jobs, self.pool.data_ptr(), out_bytes, self.check_crc, summ.data_ptr(),
+                           qws)
         csz = ctypes_sizeof(_lib.ChainSummary)
         csumm = scratch.get("csumm", csz * max(len(slices), 1))
         csumm[: csz * max(len(slices), 1)].zero_()

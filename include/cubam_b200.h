@@ -89,7 +89,7 @@ int cb_device_sm_count(void);
  * One value per key for the whole process, read by every later launch; the package's autotuner
  * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
  *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB (32 KiB)
- *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (1)
+ *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (3)
  *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 6, 7 or 8 (7)
  *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 with a 16 KiB window per
  *                          warp, 12 with an 8 KiB window, 24 with a 4 KiB window (12)
@@ -173,11 +173,10 @@ int64_t cb_inflate_lane_slots(void);
 /* ---- Inflate, form 3: the Huffman decode and the copy as two kernels (same contract as cb_inflate,
  *      replacing the same nvCOMP call, src/cubam/bgzf.py:587-611) ---------------------------------
  * k_decode decodes one member per lane (32 members per warp in lock step) into 16-bit units in a
- * token arena inside the workspace; k_copy writes each member with one warp through a 32 KiB
- * shared-memory window and checks its CRC32.  Jobs must have increasing out_off with disjoint
- * outputs (as cb_scan_members writes them); a job out of that order fails with CB_ERR_ARG, a job
- * whose arena slot does not fit the workspace with CB_ERR_CAPACITY.  out_bytes: an upper bound of
- * out_off + isize over the jobs (the size of out_base's buffer). */
+ * token arena inside the workspace (a slot of 2 isize + 8 bytes per job); k_copy writes each member
+ * with one warp through a shared-memory window (CB_PARAM_COPY_WARPS) and checks its CRC32.
+ * out_bytes: the sum of isize over the jobs (or more); a job whose slot does not fit a smaller
+ * workspace fails with CB_ERR_CAPACITY. */
 size_t cb_inflate_split_workspace_bytes(int64_t n_jobs, int64_t out_bytes);
 int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,
                      int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
