@@ -107,16 +107,18 @@ __device__ __forceinline__ uint32_t unit_match(uint32_t len, uint32_t dist) {
 }
 
 // Workspace: [0, 256) queue counters; per job 16 bytes (units u32, status u32, arena slot u64); the
-// arena after that, 256-byte aligned.  Job j's slot is the prefix sum of 2 ISIZE + 8 over the jobs
-// before it (k_slots), so the arena holds 2 sum(ISIZE) + 8 n_jobs bytes whatever the jobs' output
-// offsets are.
+// arena after that, 256-byte aligned.  Job j's slot is the prefix sum of slot_bytes over the jobs
+// before it (k_slots), so the arena holds 2 sum(ISIZE) + 16 n_jobs bytes at most, whatever the
+// jobs' output offsets are.
 constexpr size_t WS_HEAD = 256;
 constexpr size_t PER_JOB = 16;
 __host__ __device__ __forceinline__ size_t arena_offset(long long n_jobs) {
     return (WS_HEAD + PER_JOB * (size_t)n_jobs + 255) & ~(size_t)255;
 }
+// A slot's bytes: 2 ISIZE for the units and room for the last word, rounded to 8 so that every slot
+// starts 8-byte aligned (k_decode stores the units as 4-byte words).
 __host__ __device__ __forceinline__ unsigned long long slot_bytes(uint32_t isize) {
-    return 2ull * isize + 8ull;
+    return (2ull * isize + 8ull + 7ull) & ~7ull;
 }
 
 // The arena slot of every job: one CTA; thread t sums a contiguous run of jobs, a block scan joins
@@ -935,7 +937,7 @@ int launch_copy(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jo
 
 extern "C" size_t cb_inflate_split_workspace_bytes(int64_t n_jobs, int64_t out_bytes) {
     if (n_jobs < 0 || out_bytes < 0) return 0;
-    return split::arena_offset(n_jobs) + 2 * (size_t)out_bytes + 8 * (size_t)n_jobs + 16;
+    return split::arena_offset(n_jobs) + 2 * (size_t)out_bytes + 16 * (size_t)n_jobs + 16;
 }
 
 extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base,

@@ -173,7 +173,7 @@ int64_t cb_inflate_lane_slots(void);
 /* ---- Inflate, form 3: the Huffman decode and the copy as two kernels (same contract as cb_inflate,
  *      replacing the same nvCOMP call, src/cubam/bgzf.py:587-611) ---------------------------------
  * k_decode decodes one member per lane (32 members per warp in lock step) into 16-bit units in a
- * token arena inside the workspace (a slot of 2 isize + 8 bytes per job); k_copy writes each member
+ * token arena inside the workspace (a slot of 2 isize + 8 bytes per job, rounded up to 8); k_copy writes each member
  * with one warp through a shared-memory window (CB_PARAM_COPY_WARPS) and checks its CRC32.
  * out_bytes: the sum of isize over the jobs (or more); a job whose slot does not fit a smaller
  * workspace fails with CB_ERR_CAPACITY. */
