@@ -356,7 +356,7 @@ def run_ours(args):
     achieved = inflated / (inflate_ms / 1e3) / 1e9
     from cubam_b200.bgzf import inflate_form
 
-    form = inflate_form(0)  # the form the batched decode runs
+    form = inflate_form(0, n_members)  # the form the batched decode runs
     kernel = {1: "k_inflate_warp", 2: "k_inflate_lanes", 3: "k_decode + k_copy"}[form]
 
     # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)

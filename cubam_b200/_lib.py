@@ -18,7 +18,8 @@ LIB_PATH = _build.LIB
 # status codes (include/cubam_b200.h)
 OK, TRUNCATED, NO_CHAIN, CORRUPT_BLOCK, INFLATE, CRC, TOO_MANY, CAPACITY, CUDA, ARG, TIMEOUT = range(11)
 #: launch parameters (cb_set_param / cb_get_param)
-PARAM_CHAIN_TILE, PARAM_INFLATE_FORM, PARAM_DECODE_ROOT, PARAM_COPY_WARPS, PARAM_DECODE_STEPS, PARAM_DECODE_PREFETCH = range(1, 7)
+(PARAM_CHAIN_TILE, PARAM_INFLATE_FORM, PARAM_DECODE_ROOT, PARAM_COPY_WARPS, PARAM_DECODE_STEPS, PARAM_DECODE_PREFETCH,
+ PARAM_SPLIT_MIN_JOBS) = range(1, 8)
 
 
 class MemberJob(ctypes.Structure):

@@ -41,10 +41,10 @@ from cubam_b200.bgzf import (
 KERNELS = {"scan": 4, "inflate": 3, "chain": 5, "decode": 1, "tags": 1}
 
 
-def inflate_launches(form: int = 0) -> int:
+def inflate_launches(form: int = 0, n_jobs: int | None = None) -> int:
     """Kernels of one inflate call: init, the persistent grid, finish; form 3 adds the slot scan and
     splits the grid into decode and copy."""
-    return 5 if inflate_form(form) == 3 else KERNELS["inflate"]
+    return 5 if inflate_form(form, n_jobs) == 3 else KERNELS["inflate"]
 
 
 @dataclass
@@ -158,7 +158,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
         launch_inflate(all_jobs.data_ptr(), n_jobs, out.data_ptr(), total, check_crc, inflate_summ.data_ptr(), qws)
         del qws
         if counter is not None:
-            counter["launches"] = counter.get("launches", 0) + inflate_launches()
+            counter["launches"] = counter.get("launches", 0) + inflate_launches(0, n_jobs)
     if events:
         events.mark("inflated")
     chains = []
@@ -353,7 +353,8 @@ class BatchPlan:
             if self.graph is not None:
                 raise RuntimeError("the captured plan's inflate workspace is too small for this form")
             self.queue_ws = torch.empty(max(need, 512), dtype=torch.uint8, device="cuda")
-        ws = self.queue_ws if inflate_form(form) == 3 else self.queue_ws[: int(_lib.lib.cb_inflate_workspace_bytes())]
+        ws = (self.queue_ws if inflate_form(form, self.job_base[-1]) == 3
+              else self.queue_ws[: int(_lib.lib.cb_inflate_workspace_bytes())])
         launch_inflate(self.jobs.data_ptr(), self.job_base[-1], self.out.data_ptr(), self.total_out, self.check_crc,
                        self.inflate_summ.data_ptr(), ws, form)
         if events:
@@ -387,7 +388,7 @@ class BatchPlan:
         """Kernels of this library in one :meth:`launch` (the graph holds the same)."""
         chains = sum(1 for d in self.data if int(d.numel()))
         decodes = sum(1 for n in self.n_records if n)
-        return (KERNELS["scan"] * self.n_files + inflate_launches(self.form or 0) + KERNELS["chain"] * chains
+        return (KERNELS["scan"] * self.n_files + inflate_launches(self.form or 0, self.job_base[-1]) + KERNELS["chain"] * chains
                 + (KERNELS["decode"] + (KERNELS["tags"] if self.tags else 0)) * decodes)
 
     def check(self) -> None:

@@ -220,14 +220,21 @@ def scan_members(buf: torch.Tensor, eof: bool, out_base: int = 0, jobs_cap: int 
         return jobs, s
 
 
-def inflate_form(form: int = 0) -> int:
-    """The inflate form a call with ``form`` runs: 0 is the library's default (``CB_PARAM_INFLATE_FORM``)."""
-    return int(_lib.lib.cb_get_param(_lib.PARAM_INFLATE_FORM)) if form == 0 else int(form)
+def inflate_form(form: int = 0, n_jobs: int | None = None) -> int:
+    """The inflate form a call of ``n_jobs`` jobs with ``form`` runs, as ``cb_inflate_form`` chooses it:
+    0 is the library's default (``CB_PARAM_INFLATE_FORM``; form 1 in place of form 3 below
+    ``CB_PARAM_SPLIT_MIN_JOBS`` jobs)."""
+    if form:
+        return int(form)
+    f = int(_lib.lib.cb_get_param(_lib.PARAM_INFLATE_FORM))
+    if f == 3 and n_jobs is not None and n_jobs < int(_lib.lib.cb_get_param(_lib.PARAM_SPLIT_MIN_JOBS)):
+        return 1
+    return f
 
 
 def inflate_workspace_bytes(n_jobs: int, out_bytes: int, form: int = 0) -> int:
     """Workspace bytes of an inflate of ``n_jobs`` jobs writing ``out_bytes`` bytes in total, in ``form``."""
-    if inflate_form(form) == 3:
+    if inflate_form(form, n_jobs) == 3:
         return max(int(_lib.lib.cb_inflate_split_workspace_bytes(n_jobs, out_bytes)), 512)
     return int(_lib.lib.cb_inflate_workspace_bytes())
 
@@ -237,7 +244,7 @@ def launch_inflate(jobs_ptr: int, n_jobs: int, out_ptr, out_bytes: int, check_cr
     """``cb_inflate_form`` on the current stream with a workspace from :func:`inflate_workspace_bytes`
     (a workspace larger than the forms-1/2 size selects form 3 when the form asks for it)."""
     rc = _lib.lib.cb_inflate_form(jobs_ptr, n_jobs, d_n_jobs_ptr, out_ptr, int(check_crc), job_status_ptr, summary_ptr,
-                                  workspace.data_ptr(), workspace.numel(), inflate_form(form), stream_ptr())
+                                  workspace.data_ptr(), workspace.numel(), int(form), stream_ptr())
     _lib.check(rc, "cb_inflate_form")
 
 

@@ -1414,7 +1414,10 @@ extern "C" int cb_inflate_form(const cb_member_job* jobs, int64_t n_jobs, const 
                                int check_crc, uint32_t* job_status, cb_inflate_summary* summary, void* workspace,
                                size_t workspace_bytes, int form, void* stream) {
     if (!summary || !workspace || workspace_bytes < cb_inflate_workspace_bytes() || n_jobs < 0) return CB_ERR_ARG;
-    if (form == 0) form = (int)cb_param(CB_PARAM_INFLATE_FORM);
+    if (form == 0) {
+        form = (int)cb_param(CB_PARAM_INFLATE_FORM);
+        if (form == 3 && n_jobs < cb_param(CB_PARAM_SPLIT_MIN_JOBS)) form = 1;
+    }
     if (form == 3) {
         // the split form needs its token arena: a workspace of the forms-1/2 size runs form 1 instead
         if (workspace_bytes > cb_inflate_workspace_bytes())

@@ -96,6 +96,9 @@ int cb_device_sm_count(void);
  *   CB_PARAM_DECODE_STEPS  decode steps of form 3 between lane scheduling rounds: 1-64 (16)
  *   CB_PARAM_DECODE_PREFETCH  lines (128 B) of compressed input form 3's decoder asks L2 for ahead of
  *                          each lane's position: 0-16, 0 = none (4)
+ *   CB_PARAM_SPLIT_MIN_JOBS   with CB_PARAM_INFLATE_FORM 3, form 0 runs form 1 for calls of fewer jobs
+ *                          (form 3 decodes one member per lane, so it needs many members to fill the GPU):
+ *                          0 or more (40000)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
@@ -104,7 +107,8 @@ enum {
     CB_PARAM_DECODE_ROOT = 3,
     CB_PARAM_COPY_WARPS = 4,
     CB_PARAM_DECODE_STEPS = 5,
-    CB_PARAM_DECODE_PREFETCH = 6
+    CB_PARAM_DECODE_PREFETCH = 6,
+    CB_PARAM_SPLIT_MIN_JOBS = 7
 };
 int cb_set_param(int key, int64_t value);
 int64_t cb_get_param(int key);
@@ -159,7 +163,8 @@ int cb_inflate(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_job
                void* stream);
 
 /* cb_inflate with the form given: 1 = one member per warp, 2 = one member per lane (most
- * members in flight), 3 = cb_inflate_split, 0 = CB_PARAM_INFLATE_FORM.  Form 3 runs only with a
+ * members in flight), 3 = cb_inflate_split, 0 = CB_PARAM_INFLATE_FORM (form 1 in place of form 3 for
+ * fewer than CB_PARAM_SPLIT_MIN_JOBS jobs).  Form 3 runs only with a
  * workspace larger than cb_inflate_workspace_bytes() (sized by cb_inflate_split_workspace_bytes);
  * with the small workspace form 1 runs in its place.  Every form gives the same bytes and the same
  * per-job codes.  No cubam counterpart (cubam has one nvCOMP call, src/cubam/bgzf.py:595). */
