@@ -79,15 +79,15 @@ def read_struct(t: torch.Tensor, cls):
 
 
 class _ChunkReader:
-    """The chunks of a file on the device, read ahead by one background thread.
+    """The chunks of a file on the device, read ahead on the host by one background thread.
 
     The thread fills pinned host slots (``n_buffers`` of ``chunk_bytes``) in turn: a chunk is read
-    by ``n_threads`` workers with ``os.preadv`` of ``piece`` bytes each, straight into its slot,
-    then the thread issues the slot's copy to a fresh device buffer on a CUDA stream of its own and
-    records an event.  Iterating yields ``(chunk, eof)``: the consumer's current stream waits on
-    the copy's event (no host wait), so the copies of the chunks ahead run under the kernels of
-    the current one.  A slot is refilled once the copy out of it has completed, and at most
-    ``n_buffers`` chunks are read ahead of the consumer.
+    by ``n_threads`` workers with ``os.preadv`` of ``piece`` bytes each, straight into its slot.
+    Iterating yields ``(chunk, eof)`` with the chunk on the device; the copy of the NEXT chunk is
+    issued (on a stream of its own, into memory of the consumer's stream) before the current one is
+    yielded, so it runs under the kernels the consumer launches for the current one; the consumer's
+    stream waits on the copy's event, never the host.  A slot is refilled once the copy out of it
+    has completed, and the thread reads at most ``n_buffers`` chunks ahead.
 
     An exception in the thread (an unreadable file, a short read) reaches the consumer at the first
     chunk it has not delivered.  Without CUDA the chunks are host tensors (no pinned memory, no
@@ -98,11 +98,11 @@ class _ChunkReader:
         self.path, self.chunk = Path(path), int(chunk_bytes)
         self.n_buffers, self.n_threads, self.piece = max(int(n_buffers), 1), max(int(n_threads), 1), max(int(piece), 1)
         self._cuda = torch.cuda.is_available()
-        self._device = torch.cuda.current_device() if self._cuda else None
         self._slots = [torch.empty(self.chunk, dtype=torch.uint8, pin_memory=self._cuda) for _ in range(self.n_buffers)]
         self._cv = threading.Condition()
-        self._ready: dict[int, tuple] = {}  # chunk index -> (tensor, eof, event)
-        self._delivered = 0                  # chunks handed to the consumer
+        self._ready: dict[int, tuple] = {}         # chunk index -> (slot, nbytes, eof), read by the thread
+        self._copied: list = [None] * self.n_buffers  # event of the last copy out of each slot
+        self._taken = 0                              # chunks the consumer has taken from the thread
         self._failure: BaseException | None = None
         self._closed = False
         self._thread = threading.Thread(target=self._produce, name="cubam-reader", daemon=True)
@@ -126,44 +126,31 @@ class _ChunkReader:
         from concurrent.futures import ThreadPoolExecutor
 
         try:
-            if self._cuda:
-                torch.cuda.set_device(self._device)
-                stream = torch.cuda.Stream()
-            copied: list = [None] * self.n_buffers  # event of the last copy out of each slot
             fd = os.open(self.path, os.O_RDONLY)
             try:
                 size = os.fstat(fd).st_size
                 with ThreadPoolExecutor(self.n_threads) as workers:
                     k = off = 0
                     while True:
+                        slot = k % self.n_buffers
                         with self._cv:
-                            while not self._closed and k - self._delivered >= self.n_buffers:
+                            while not self._closed and k - self._taken >= self.n_buffers:
                                 self._cv.wait()
                             if self._closed:
                                 return
-                        slot = k % self.n_buffers
-                        if copied[slot] is not None:
-                            copied[slot].synchronize()  # the slot's previous chunk has left it
+                            ev = self._copied[slot]
+                        if ev is not None:
+                            ev.synchronize()  # the copy out of this slot has completed
                         n = min(self.chunk, size - off)
                         view = memoryview(self._slots[slot].numpy())[:n]
                         reads = [workers.submit(self._read_piece, fd, view[p : p + self.piece], off + p)
                                  for p in range(0, n, self.piece)]
                         for r in reads:
                             r.result()
-                        ev = None
-                        if self._cuda:
-                            with torch.cuda.stream(stream):
-                                chunk = torch.empty(n, dtype=torch.uint8, device=self._device)
-                                chunk.copy_(self._slots[slot][:n], non_blocking=True)
-                                ev = torch.cuda.Event()
-                                ev.record(stream)
-                            copied[slot] = ev
-                        else:
-                            chunk = self._slots[slot][:n].clone()
                         off += n
                         eof = off >= size
                         with self._cv:
-                            self._ready[k] = (chunk, eof, ev)
+                            self._ready[k] = (slot, n, eof)
                             self._cv.notify_all()
                         if eof:
                             return
@@ -175,24 +162,52 @@ class _ChunkReader:
                 self._failure = e
                 self._cv.notify_all()
 
-    def __iter__(self) -> Iterator[tuple[torch.Tensor, bool]]:
-        k = 0
-        while True:
+    def _take(self, k: int) -> tuple:
+        with self._cv:
+            while k not in self._ready and self._failure is None:
+                self._cv.wait()
+            if k not in self._ready:
+                raise self._failure  # type: ignore[misc]
+            return self._ready.pop(k)
+
+    def _upload(self, k: int, stream) -> tuple:
+        """Chunk k on the device: its copy issued on ``stream``; (tensor, eof, event)."""
+        slot, n, eof = self._take(k)
+        if not self._cuda:
+            chunk = self._slots[slot][:n].clone()
             with self._cv:
-                while k not in self._ready and self._failure is None:
-                    self._cv.wait()
-                if k not in self._ready:
-                    raise self._failure  # type: ignore[misc]
-                chunk, eof, ev = self._ready.pop(k)
-                self._delivered = k + 1
+                self._taken = k + 1
                 self._cv.notify_all()
+            return chunk, eof, None
+        chunk = torch.empty(n, dtype=torch.uint8, device="cuda")  # memory of the consumer's stream
+        stream.wait_stream(torch.cuda.current_stream())  # the memory may have been in use there
+        with torch.cuda.stream(stream):
+            chunk.copy_(self._slots[slot][:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        with self._cv:
+            self._copied[slot] = ev
+            self._taken = k + 1
+            self._cv.notify_all()
+        return chunk, eof, ev
+
+    def __iter__(self) -> Iterator[tuple[torch.Tensor, bool]]:
+        stream = torch.cuda.Stream() if self._cuda else None
+        k = 0
+        cur = self._upload(0, stream)
+        while cur is not None:
+            chunk, eof, ev = cur
+            failure = None
+            try:
+                cur = None if eof else self._upload(k + 1, stream)  # the next copy runs under this chunk's work
+            except BaseException as e:  # noqa: BLE001  (raised after the chunk read before it)
+                cur, failure = None, e
             if ev is not None:
-                cur = torch.cuda.current_stream()
-                cur.wait_event(ev)
-                chunk.record_stream(cur)  # allocated on the reader's stream, used on this one
+                torch.cuda.current_stream().wait_event(ev)
             yield chunk, eof
-            if eof:
-                return
+            del chunk
+            if failure is not None:
+                raise failure
             k += 1
 
 

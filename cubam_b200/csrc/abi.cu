@@ -30,7 +30,7 @@ struct Param {
     int64_t lo, hi, def;
 };
 constexpr Param kParams[] = {
-    {CB_PARAM_CHAIN_TILE, 2048, 1 << 22, 32768},
+    {CB_PARAM_CHAIN_TILE, 0, 1 << 22, 0},
     {CB_PARAM_INFLATE_FORM, 1, 3, 3},
     {CB_PARAM_DECODE_ROOT, 6, 8, 7},
     {CB_PARAM_COPY_WARPS, 2, 24, 12},
@@ -66,8 +66,8 @@ extern "C" int cb_set_param(int key, int64_t value) {
     }
     if (value < kParams[i].lo || value > kParams[i].hi)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
-    if (key == CB_PARAM_CHAIN_TILE && (value & (value - 1)))
-        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is a power of two");
+    if (key == CB_PARAM_CHAIN_TILE && value && (value < 2048 || (value & (value - 1))))
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two >= 2048");
     if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6 && value != 12 && value != 24)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3, 6, 12 or 24");
     g_param[i].store(value, std::memory_order_relaxed);

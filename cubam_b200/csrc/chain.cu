@@ -6,7 +6,7 @@
 // follows block_size while the predicate holds, which is O(records), not O(bytes).  It is walked in
 // parallel by tiles:
 //
-//  1. k_walk: one thread per tile (CB_PARAM_CHAIN_TILE bytes, 32 KB unless tuned) finds the tile's first offset that passes the predicate and
+//  1. k_walk: one thread per tile (CB_PARAM_CHAIN_TILE bytes; by default 2-32 KB from the data size) finds the tile's first offset that passes the predicate and
 //     walks the block_size links from it (each record checked with the full predicate) up to the first
 //     offset past the tile: first[t], count[t], exit[t], and whether the walk broke inside the tile.
 //  2. k_check: tile t's walk is the true chain when its first offset is where the previous non-empty
@@ -281,7 +281,15 @@ extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, in
     if (n < 0 || !summary || !workspace || (n > 0 && (!data || !offsets)) || cap < 0) return CB_ERR_ARG;
     if (workspace_bytes < chain::ws_bytes(n)) return CB_ERR_CAPACITY;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    chain::Ws w = chain::carve(workspace, n, cb_param(CB_PARAM_CHAIN_TILE));
+    long long tile = cb_param(CB_PARAM_CHAIN_TILE);
+    if (tile == 0) {
+        // about one walk per thread that the GPU keeps resident (1,024 per SM): big enough tiles for the
+        // first-candidate search to be rare, enough of them for the dependent loads to overlap
+        const long long want = n / ((long long)cb_device_sm_count() * 1024);
+        tile = chain::T_MIN;
+        while (tile < 32768 && tile * 2 <= want) tile *= 2;
+    }
+    chain::Ws w = chain::carve(workspace, n, tile);
     const long long sms = cb_device_sm_count();
     long long grid = (w.ntiles + chain::NT - 1) / chain::NT;
     if (grid > sms * 16) grid = sms * 16;

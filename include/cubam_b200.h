@@ -88,7 +88,8 @@ int cb_device_sm_count(void);
  *      src/cubam/_memory.py:11-23) ---------------------------------------------------------------
  * One value per key for the whole process, read by every later launch; the package's autotuner
  * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
- *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB (32 KiB)
+ *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB, or 0:
+ *                          chosen from the data size, about one tile per resident thread, 2-32 KiB (0)
  *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (3)
  *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 6, 7 or 8 (7)
  *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 with a 16 KiB window per
