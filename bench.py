@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--file-records", type=int, default=4_000_000, help="serve: records per resident file")
     ap.add_argument("--scale", type=float, default=1.0, help="uneven: record counts times this")
     ap.add_argument("--records", type=int, default=None, help="override the workload size (records)")
-    ap.add_argument("--chunk-bytes", type=int, default=256 << 20, help="compressed chunk of the e2e read_bam")
+    ap.add_argument("--chunk-bytes", type=int, default=None,
+                    help="compressed chunk of the e2e read_bam (default: read_bam's own, auto_chunk_bytes())")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-sample-mb", type=int, default=2048, help="compressed MB of the CPU baseline sample")
     ap.add_argument("--workdir", default=None)
@@ -362,7 +363,7 @@ def run_ours(args):
     # the plain per-chunk form of the same kernels on device-resident chunks (cubam's structure)
     plain = None
     if not args.no_plain:
-        plain = plain_per_chunk(comp, header, args.chunk_bytes, tags)
+        plain = plain_per_chunk(comp, header, args.chunk_bytes or (256 << 20), tags)
 
     fused = fused_record_pass(comp, header) if rank == 0 else None
 
@@ -541,11 +542,14 @@ def run_e2e(path, args, tags, inflated, rank, dist):
     import cubam_b200
 
     size = os.path.getsize(path)
+    from cubam_b200 import auto_chunk_bytes
+
+    chunk = args.chunk_bytes or auto_chunk_bytes()
 
     def one():
         chk = torch.zeros(1, dtype=torch.int64, device="cuda")
         recs = 0
-        for b in cubam_b200.read_bam(path, chunk_bytes=args.chunk_bytes):
+        for b in cubam_b200.read_bam(path, chunk_bytes=chunk):
             for t in b.tags(*tags):
                 chk += t.length.sum()
             chk += b.pos.sum()
@@ -578,7 +582,7 @@ def run_e2e(path, args, tags, inflated, rank, dist):
         "ms_per_step": ms,
         "wall_ms_per_step": wall * 1e3,
         "records_per_s": recs * world / (ms / 1e3),
-        "chunk_bytes": args.chunk_bytes,
+        "chunk_bytes": chunk,
         "api": "cubam_b200.read_bam(path) + RecordBatch.tags('CB','UB','GN')",
     }
 

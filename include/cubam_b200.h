@@ -99,7 +99,7 @@ int cb_device_sm_count(void);
  *                          each lane's position: 0-16, 0 = none (4)
  *   CB_PARAM_SPLIT_MIN_JOBS   with CB_PARAM_INFLATE_FORM 3, form 0 runs form 1 for calls of fewer jobs
  *                          (form 3 decodes one member per lane, so it needs many members to fill the GPU):
- *                          0 or more (40000)
+ *                          0 or more (30000)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
