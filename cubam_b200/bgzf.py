@@ -94,7 +94,7 @@ class _ChunkReader:
     stream), which is how the reading logic is tested on a host without a GPU.
     """
 
-    def __init__(self, path, chunk_bytes: int, *, n_buffers: int = 3, n_threads: int = 8, piece: int = 16 << 20):
+    def __init__(self, path, chunk_bytes: int, *, n_buffers: int = 3, n_threads: int = 16, piece: int = 16 << 20):
         self.path, self.chunk = Path(path), int(chunk_bytes)
         self.n_buffers, self.n_threads, self.piece = max(int(n_buffers), 1), max(int(n_threads), 1), max(int(piece), 1)
         self._cuda = torch.cuda.is_available()

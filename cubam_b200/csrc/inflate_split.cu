@@ -560,7 +560,12 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 uint32_t dbase, dext;
                 dist_code(d & 31u, dbase, dext);
                 const uint32_t dist = dbase + ((y >> dl) & ((1u << dext) - 1u));
-                const uint32_t k = n1 + (is_len ? dl + dext : 0u);  // <= 48
+                // a literal may take the next code too when it is a literal of the root table: at most 15
+                // bits went to the first, and bb holds 33 or more (the step's second symbol)
+                const uint32_t xb = (uint32_t)(bb >> L);
+                const uint32_t eb = my_lit[xb & C::LMASK];
+                const bool two = is_lit && eb < 0x1000u && pos + 1 < isize;
+                const uint32_t k = n1 + (is_len ? dl + dext : two ? e_len(eb) : 0u);  // <= 48
                 if (k < bc) {
                     consume(k);
                 } else {  // the step used bits of p0: it becomes the buffer
@@ -576,8 +581,9 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 if (bad) {
                     fail(CB_ERR_INFLATE);
                 } else {
-                    put(is_len ? unit_match(len, dist) : (e & 255u), is_len ? 2u : is_lit ? 1u : 0u);
-                    pos += is_len ? len : is_lit ? 1u : 0u;
+                    put(is_len ? unit_match(len, dist) : two ? ((e & 255u) | ((eb & 255u) << 16)) : (e & 255u),
+                        is_len ? 2u : two ? 2u : is_lit ? 1u : 0u);
+                    pos += is_len ? len : two ? 2u : is_lit ? 1u : 0u;
                     if (is_eob) st = final_block ? S_FIN : S_HDR;
                 }
             } else if (st == S_CLENS) {

@@ -148,7 +148,7 @@ def test_header_errors_and_round_trip(tmp_path):
 
 def test_auto_chunk_bytes_follows_the_reference_policy(monkeypatch):
     """cubam's rule (src/cubam/_memory.py:11-23): halve while 64 chunks do not fit the free GPU memory,
-    never below 32 MB; the same sizes as cubam below 32 GB free, up to 2 GB on a B200."""
+    never below 32 MB; the same sizes as cubam below 32 GB free, up to 1 GB on a B200."""
     import torch
 
     from cubam_b200 import auto_chunk_bytes, memory_pool
@@ -156,7 +156,7 @@ def test_auto_chunk_bytes_follows_the_reference_policy(monkeypatch):
     GB, MB = 1 << 30, 1 << 20
     # free memory of an 8, 12, 16 and 24 GB GPU (cubam's docstring: about 64, 128, 128 and 256 MB)
     for free, want in ((7.5 * GB, 64 * MB), (11.5 * GB, 128 * MB), (15.5 * GB, 128 * MB), (23 * GB, 256 * MB),
-                       (1 * GB, 32 * MB), (60 * GB, 512 * MB), (178 * GB, 2 * GB)):
+                       (1 * GB, 32 * MB), (60 * GB, 512 * MB), (178 * GB, 1 * GB)):
         monkeypatch.setattr(torch.cuda, "mem_get_info", lambda free=free: (free, 2 * free))
         assert auto_chunk_bytes() == want, free
     with memory_pool():
