@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--form", type=int, default=0,
+                    help="inflate form for every batch size (1 warp per member, 2 lane per member, 3 split); "
+                         "0: the library's choice")
     return ap.parse_args()
 
 
@@ -306,7 +309,11 @@ def run_ours(args):
     cfg, n, path, gen_s = ensure_file(args, rank, dist)
 
     import cubam_b200
-    from cubam_b200 import batch
+    from cubam_b200 import _lib, batch
+
+    if args.form:
+        _lib.lib.cb_set_param(_lib.PARAM_INFLATE_FORM, args.form)
+        _lib.lib.cb_set_param(_lib.PARAM_SPLIT_MIN_JOBS, 0)
 
     header = cubam_b200.BamHeader.read(path)
     comp = batch.load_compressed(path)

@@ -593,7 +593,12 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 const uint32_t L = e_len(e), s = e & 255u;
                 const uint32_t eb = s < 16 ? 0u : s == 16 ? 2u : s == 17 ? 3u : 7u;
                 const uint32_t rep = s < 16 ? 1u : (s == 18 ? 11u : 3u) + ((x >> L) & ((1u << eb) - 1u));
-                consume(L + eb);
+                // a second plain length in the same step when its code follows (14 bits at most went to
+                // the first, bb holds 33 or more)
+                const uint32_t e2 = my_cltab[(uint32_t)(bb >> (L + eb)) & 127u];
+                const uint32_t s2 = e2 & 255u, L2 = e_len(e2);
+                const bool two = e_kind(e2) == E_CL && !(e2 & 0x8000u) && L2 != 0 && s2 < 16 && ci + rep < total;
+                consume(L + eb + (two ? L2 : 0u));
                 if (e_kind(e) != E_CL || (e & 0x8000u) || L == 0 || (s == 16 && ci == 0) || ci + rep > total) {
                     fail(CB_ERR_INFLATE);
                 } else {
@@ -604,6 +609,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                         for (uint32_t r = 0; r < rep; r++) my_lens[ci + r] = v;  // 3-6 copies
                     }
                     ci += rep;
+                    if (two) my_lens[ci++] = (uint8_t)s2;
                     if (ci == total) {
                         if (my_lens[256] == 0) fail(CB_ERR_INFLATE);  // no end-of-block code
                         else st = S_BUILD;
