@@ -305,6 +305,19 @@ __device__ __forceinline__ uint32_t load_word(const uint32_t* wbase, uint32_t nv
     return w < nvalid ? __ldg(wbase + w) : 0u;
 }
 
+// Block k (16 bytes, words 4k..4k+3) of a lane's input: one 16-byte load when the whole block lies
+// within the nvalid readable words, else word by word (zero past the end).
+__device__ __forceinline__ uint4 load_block(const uint32_t* base16, uint32_t nvalid, uint32_t k) {
+    const uint32_t w = 4 * k;
+    if (w + 3 < nvalid) return __ldg(reinterpret_cast<const uint4*>(base16) + k);
+    uint4 v;
+    v.x = w < nvalid ? __ldg(base16 + w) : 0u;
+    v.y = w + 1 < nvalid ? __ldg(base16 + w + 1) : 0u;
+    v.z = w + 2 < nvalid ? __ldg(base16 + w + 2) : 0u;
+    v.w = w + 3 < nvalid ? __ldg(base16 + w + 3) : 0u;
+    return v;
+}
+
 // A hint to bring the 128-byte line of p into L2 (a prefetch, no load into registers).
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
@@ -335,10 +348,13 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     // the member of this lane
     int st = S_IDLE;
     long long j = 0;
-    // bit reader: bb holds bc bits (LSB first); p0, p1 are the next two words, nw the word after them
-    const uint32_t* wbase = nullptr;
+    // bit reader: bb holds bc bits (LSB first), fed from registers: a0-a3 the words left of the current
+    // 16-byte block (acnt of them, a0 next), blk the next block, loaded a block ahead (nb: the block
+    // after it); wfed words went into bb so far
+    const uint32_t* wbase = nullptr;  // 16-byte aligned start at or before the payload
     uint64_t bb = 0;
-    uint32_t bc = 0, p0 = 0, p1 = 0, nw = 0, nvalid = 0;
+    uint32_t bc = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, acnt = 0, nb = 0, wfed = 0, nvalid = 0;
+    uint4 blk = make_uint4(0, 0, 0, 0);
     uint32_t s0 = 0, in_bits = 0, isize = 0, pos = 0;
     bool final_block = false;
     uint32_t rem = 0, hlit = 0, total = 0, ci = 0;  // stored bytes left; code lengths read
@@ -351,23 +367,36 @@ __global__ void __launch_bounds__(C::WARPS * 32)
 #pragma unroll
     for (int i = 0; i < C::NLD; i++) dlim[i] = 0;
 
+    auto next_word = [&]() {  // a0 went into bb: the next word becomes a0
+        a0 = a1;
+        a1 = a2;
+        a2 = a3;
+        wfed++;
+        if (--acnt == 0) {
+            a0 = blk.x;
+            a1 = blk.y;
+            a2 = blk.z;
+            a3 = blk.w;
+            acnt = 4;
+            blk = load_block(wbase, nvalid, nb);
+            // entering a new 128-byte line of input: ask L2 for the line `ahead` lines further on, so
+            // that the block loads find the lane's stream in L2 rather than DRAM
+            if (ahead && (nb & 7u) == 0 && 4 * (nb + 8 * ahead) < nvalid) prefetch_l2(wbase + 4 * (nb + 8 * ahead));
+            nb++;
+        }
+    };
     auto refill = [&]() {  // afterwards bc >= 33
         if (bc <= 32) {
-            bb |= (uint64_t)p0 << bc;
+            bb |= (uint64_t)a0 << bc;
             bc += 32;
-            p0 = p1;
-            p1 = load_word(wbase, nvalid, nw);
-            // entering a new 128-byte line of input: ask L2 for the line `ahead` lines further on, so
-            // that the lane's loads find its stream in L2 rather than DRAM
-            if (ahead && (nw & 31u) == 0 && nw + ahead * 32 < nvalid) prefetch_l2(wbase + nw + ahead * 32);
-            nw++;
+            next_word();
         }
     };
     auto consume = [&](uint32_t k) {  // k <= bc
         bb >>= k;
         bc -= k;
     };
-    auto consumed = [&]() { return (nw - 2) * 32u - bc - s0; };  // bits of the payload used
+    auto consumed = [&]() { return wfed * 32u - bc - s0; };  // bits of the payload used
     auto put = [&](uint32_t v, uint32_t k) {  // append k (0, 1 or 2) units, packed low unit first
         if (k) {
             const uint32_t wv = has ? (half | (v << 16)) : v;
@@ -397,19 +426,26 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 } else {
                     const cb_member_job job = jobs[j];
                     const uintptr_t in = (uintptr_t)job.in;
-                    wbase = reinterpret_cast<const uint32_t*>(in & ~(uintptr_t)3);
-                    s0 = (uint32_t)(in & 3) * 8;
+                    wbase = reinterpret_cast<const uint32_t*>(in & ~(uintptr_t)15);
+                    s0 = (uint32_t)(in & 15) * 8;  // bits of the first block before the payload
                     nvalid = (uint32_t)((in + job.in_len + 8 - (uintptr_t)wbase) >> 2);
                     in_bits = job.in_len * 8u;
                     isize = job.isize;
                     bb = 0;
                     bc = 0;
-                    p0 = load_word(wbase, nvalid, 0);
-                    p1 = load_word(wbase, nvalid, 1);
-                    nw = 2;
+                    wfed = 0;
+                    const uint4 b0 = load_block(wbase, nvalid, 0);
+                    a0 = b0.x;
+                    a1 = b0.y;
+                    a2 = b0.z;
+                    a3 = b0.w;
+                    acnt = 4;
+                    blk = load_block(wbase, nvalid, 1);
+                    nb = 2;
+                    for (uint32_t q = 0; q < (s0 >> 5); q++) next_word();  // whole words before the payload
                     refill();
                     refill();
-                    consume(s0);
+                    consume(s0 & 31u);
                     pos = 0;
                     final_block = false;
                     nunits = nwords = half = has = 0;
@@ -551,9 +587,9 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 const uint32_t len = (e & 255u) + 3 + ((x >> L) & ((1u << ext) - 1u));
                 const uint32_t n1 = L + ext;  // <= 20 < bc
                 // the distance (used by lengths only) from the 32 bits after n1: the rest of bb and,
-                // past its bc bits, the next word -- no refill inside the step
+                // past its bc bits, the next word a0 -- no refill inside the step
                 const uint32_t avail = bc - n1;
-                const uint32_t y = (uint32_t)(bb >> n1) | (avail < 32 ? p0 << avail : 0u);
+                const uint32_t y = (uint32_t)(bb >> n1) | (avail < 32 ? a0 << avail : 0u);
                 uint32_t d = my_dist[y & C::DMASK];
                 if (is_len && d == E_LONG) d = long_entry<C::NLD, 32>(y, dlim, my_dsym);
                 const uint32_t dl = e_len(d);
@@ -568,13 +604,11 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 const uint32_t k = n1 + (is_len ? dl + dext : two ? e_len(eb) : 0u);  // <= 48
                 if (k < bc) {
                     consume(k);
-                } else {  // the step used bits of p0: it becomes the buffer
+                } else {  // the step used bits of a0: it becomes the buffer
                     const uint32_t r = k - bc;  // < 16
-                    bb = (uint64_t)(p0 >> r);
+                    bb = (uint64_t)(a0 >> r);
                     bc = 32 - r;
-                    p0 = p1;
-                    p1 = load_word(wbase, nvalid, nw);
-                    nw++;
+                    next_word();
                 }
                 const bool bad = (!is_len && !is_lit && !is_eob) || (is_lit && pos >= isize) ||
                                  (is_len && (e_kind(d) != E_DIST || (d & 0x8000u) || dist > pos || len > isize - pos));
