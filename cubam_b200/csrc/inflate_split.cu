@@ -682,7 +682,6 @@ struct CopyCfg {
         uint32_t crc8[8][256];
         uint32_t mulk[4][256];   // x * x^(8 (WIN - 32)) by bytes: moves a column past the other lanes
         uint32_t tok[WARPS_][32];  // the tokens of the warp's current group, in order
-        uint32_t tokq[WARPS_][32]; // their start within the group | length << 16
         alignas(16) uint8_t ring[WARPS_][RING_];
     };
 };
@@ -776,7 +775,6 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint8_t* ring = S.ring[warp];
     uint32_t* tokw = S.tok[warp];
-    uint32_t* tokq = S.tokq[warp];
     const uint32_t incl = lane == 31 ? 0xFFFFFFFFu : (2u << lane) - 1u;  // lanes 0..lane
     unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + 1;
     const uint32_t* per_job = reinterpret_cast<const uint32_t*>(ws + WS_HEAD);
@@ -836,18 +834,17 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             // the group's tokens in order (tails are not tokens): literal byte, or 0x80000000 | distance
             const bool is_tok = len != 0;
             const unsigned tokmask = __ballot_sync(FULL, is_tok);
-            if (is_tok) {
-                const uint32_t o = __popc(tokmask & ((1u << lane) - 1u));
-                tokw[o] = is_head ? (0x80000000u | dist) : (u & 255u);
-                tokq[o] = ex | (len << 16);
-            }
+            if (is_tok) tokw[__popc(tokmask & ((1u << lane) - 1u))] = is_head ? (0x80000000u | dist) : (u & 255u);
             __syncwarp();
+            // a token starts in round ex >> 5 of the group, at bit ex & 31 of that round's start mask
+            const uint32_t my_round = is_tok ? ex >> 5 : 0xFFFFFFFFu, my_bit = 1u << (ex & 31u);
             uint32_t before = 0;  // tokens that start before this round
-            for (uint32_t r0 = 0; r0 < glen; r0 += 32) {
+            uint32_t ri = 0;
+            for (uint32_t r0 = 0; r0 < glen; r0 += 32, ri++) {
                 const uint32_t rel = r0 + lane;
                 // the token of byte rel: tokens starting in this round set bits of a mask; the byte's
                 // token is the last one starting at or before it
-                const uint32_t sm = __reduce_or_sync(FULL, (is_tok && ex >= r0 && ex < r0 + 32) ? 1u << (ex - r0) : 0u);
+                const uint32_t sm = __reduce_or_sync(FULL, my_round == ri ? my_bit : 0u);
                 const uint32_t ord = before + __popc(sm & incl) - 1;
                 before += __popc(sm);
                 const uint32_t t = tokw[ord & 31u];
@@ -855,19 +852,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 uint32_t val = t & 255u;
                 int src = lane;  // the lane of this round holding the byte's source
                 if (rel < glen && (t & 0x80000000u)) {
-                    const uint32_t d = t & 0x7FFFFFFFu;
-                    uint32_t x = b - d;
-                    const uint32_t tq = tokq[ord & 31u], q = p + (tq & 0xFFFFu);
-                    if (x >= q) {
-                        // an overlapping match repeats the d bytes before it: take the byte one period
-                        // back from the token's start, x = q - d + (b - q) mod d
-                        const uint32_t m = b - q;
-                        uint32_t k = (uint32_t)((float)m * __frcp_rn((float)d));
-                        int r = (int)m - (int)(k * d);
-                        if (r < 0) r += (int)d;
-                        if (r >= (int)d) r -= (int)d;
-                        x = q - d + (uint32_t)r;
-                    }
+                    const uint32_t x = b - (t & 0x7FFFFFFFu);
                     if (x >= p + r0) src = (int)(x - (p + r0));
                     else if (x + C::RING >= p + r0 + 32) val = ring[(x + a) & C::RMASK];
                     else val = __ldcg(out + x);  // flushed long ago (the ring keeps the last RING - 32 bytes)
