@@ -85,6 +85,7 @@ _SIGNATURES = {
     "cb_inflate_split": (c_int, [P, I64, P, P, c_int, P, P, P, c_size_t, P]),
     "cb_record_chain_workspace_bytes": (c_size_t, [I64]),
     "cb_record_chain": (c_int, [P, I64, c_int32, P, I64, P, P, c_size_t, P]),
+    "cb_first_record": (c_int, [P, I64, c_int32, I64, c_int32, P, P]),
     "cb_decode_fixed": (c_int, [P, P, I64] + [P] * 11 + [P]),
     "cb_decode_records": (c_int, [P, P, I64] + [P] * 13 + [P]),
     "cb_find_tags": (c_int, [P, P, I64, c_char_p, c_int32, P, P, P, P, P]),

@@ -267,6 +267,38 @@ __global__ void k_finish(long long n, Ws w, long long cap, cb_chain_summary* sum
     summary->status = w.meta[3] > cap ? CB_ERR_CAPACITY : CB_OK;
 }
 
+// The first offset below `limit` where a record passes the predicate and the next `hops` records
+// (following block_size) pass it too, or the data ends on the way (a record that runs past the end is
+// taken as the start of an incomplete one): the speculative start of a shard's first record.
+__global__ void __launch_bounds__(NT) k_first(const uint8_t* b, long long n, int n_ref, long long limit, int hops,
+                                              unsigned long long* best) {
+    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < limit;
+         o += (long long)gridDim.x * blockDim.x) {
+        if ((unsigned long long)o >= *(volatile unsigned long long*)best) break;
+        if (o + 4 > n) break;
+        const uint32_t bs = ld_u32(b, o);
+        if (bs - 33u > (1u << 22) - 33u) continue;
+        if (!is_record(b, n, o, n_ref)) continue;
+        long long q = o + 4 + (long long)bs;
+        bool ok = true;
+        for (int h = 0; h < hops && q + 4 <= n; h++) {
+            const uint32_t bq = ld_u32(b, q);
+            if (q + 4 + (long long)bq > n) {  // runs past the end: an incomplete record, if plausible
+                ok = bq >= 33u && bq <= (1u << 22);
+                break;
+            }
+            if (!is_record(b, n, q, n_ref)) {
+                ok = false;
+                break;
+            }
+            q += 4 + (long long)bq;
+        }
+        if (ok) atomicMin(best, (unsigned long long)o);
+    }
+}
+
+__global__ void k_first_init(unsigned long long* best) { *best = ~0ull; }
+
 }  // namespace chain
 }  // namespace cb
 
@@ -305,5 +337,21 @@ extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, in
         chain::k_serial<<<1, 1, 0, s>>>(data, n, n_ref, w, offsets, cap, summary);
     }
     chain::k_finish<<<1, 1, 0, s>>>(n, w, cap, summary);
+    return cb_set_error(cudaGetLastError());
+}
+
+extern "C" int cb_first_record(const uint8_t* data, int64_t n, int32_t n_ref, int64_t limit, int32_t hops,
+                               int64_t* first, void* stream) {
+    if (n < 0 || limit < 0 || hops < 0 || !first || (n > 0 && !data)) return CB_ERR_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    unsigned long long* best = reinterpret_cast<unsigned long long*>(first);
+    chain::k_first_init<<<1, 1, 0, s>>>(best);
+    const long long lim = limit < n ? limit : n;
+    if (lim > 0) {
+        long long grid = (lim + chain::NT - 1) / chain::NT;
+        const long long cap = (long long)cb_device_sm_count() * 8;
+        if (grid > cap) grid = cap;
+        chain::k_first<<<(unsigned)grid, chain::NT, 0, s>>>(data, n, n_ref, lim, hops, best);
+    }
     return cb_set_error(cudaGetLastError());
 }

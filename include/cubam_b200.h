@@ -201,6 +201,15 @@ size_t cb_record_chain_workspace_bytes(int64_t n);
 int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, int64_t* offsets, int64_t cap,
                     cb_chain_summary* summary, void* workspace, size_t workspace_bytes, void* stream);
 
+/* The speculative start of the first record of a shard of a file's records (no counterpart in cubam,
+ * which reads a file on one GPU from its start, src/cubam/bam.py:421-446): the first offset o < limit
+ * where the record predicate holds and holds for the next `hops` records reached by block_size (or the
+ * data ends on the way).  *first (device int64) gets o, or -1 when there is none.  A rank of a
+ * sharded decode chains from there while the previous rank is still working, and checks the start
+ * once the previous rank's incomplete-record tail arrives. */
+int cb_first_record(const uint8_t* data, int64_t n, int32_t n_ref, int64_t limit, int32_t hops, int64_t* first,
+                    void* stream);
+
 /* ---- Columns: replaces decode_fixed (src/cubam/_kernels.py:292-319, src/cubam/bam.py:269-288) ---- */
 
 int cb_decode_fixed(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,

@@ -52,3 +52,19 @@ def test_shards_equal_the_whole_file(paths, world):
 def _size(p, i):
     o = int(p.offset[i].item())
     return 4 + int.from_bytes(p.data[o : o + 4].cpu().numpy().tobytes(), "little")
+
+
+def test_shards_with_a_header_of_many_members(tmp_path):
+    """A header spread over ~150 BGZF members (3,000 extra references) and 7 ranks: no rank but the
+    first starts inside it, and the shards give the whole file's records."""
+    from test_shard_host import _big_header_bam
+
+    p, _ = _big_header_bam(tmp_path)
+    header = BamHeader.read(p)
+    whole = batch.decode_many([(batch.load_compressed(p), header)], tags=TAGS)[0]
+    for world in (2, 7):
+        parts = shard.decode_shards_in_turn(p, world, tags=TAGS)
+        assert sum(len(x) for x in parts) == len(whole)
+        for k in FIELDS:
+            got = torch.cat([x.columns[k] for x in parts])
+            assert torch.equal(got, whole.columns[k]), k

@@ -82,3 +82,45 @@ def test_tails_pass_from_rank_to_rank_over_gloo():
         assert p.exitcode == 0
     got = dict(q.get(timeout=10) for _ in range(3))
     assert got == {0: b"", 1: b"tail-of-0", 2: b"tail-of-1" * 2}
+
+
+def _big_header_bam(tmp_path, member_bytes=700, extra_refs=3000):
+    """A golden BAM rewritten with ``extra_refs`` more references in its header, in small members: the
+    header spans many BGZF members."""
+    import gzip
+
+    raw = gzip.decompress((GOLDEN / "mixed_b700.bam").read_bytes())
+    l_text = struct.unpack_from("<i", raw, 4)[0]
+    n_ref = struct.unpack_from("<i", raw, 8 + l_text)[0]
+    o = 12 + l_text
+    refs = []
+    for _ in range(n_ref):
+        ln = struct.unpack_from("<i", raw, o)[0]
+        refs.append(raw[o : o + 8 + ln])
+        o += 8 + ln
+    records = raw[o:]
+    extra = [struct.pack("<i", 12) + b"extra%06d\0" % i + struct.pack("<i", 1000 + i) for i in range(extra_refs)]
+    text = raw[8 : 8 + l_text] + b"".join(b"@SQ\tSN:extra%06d\tLN:%d\n" % (i, 1000 + i) for i in range(extra_refs))
+    head = b"BAM\1" + struct.pack("<i", len(text)) + text + struct.pack("<i", n_ref + extra_refs) + b"".join(refs + extra)
+    blob = head + records
+    members = [_member(blob[i : i + member_bytes], 6) for i in range(0, len(blob), member_bytes)]
+    p = tmp_path / "bighead.bam"
+    p.write_bytes(b"".join(members) + _member(b""))
+    return p, len(head)
+
+
+def test_no_shard_but_the_first_starts_inside_the_header(tmp_path):
+    p, hsize = _big_header_bam(tmp_path)
+    raw = p.read_bytes()
+    first_ok = shard.records_start_member(raw, hsize)
+    # the header's members: their ISIZE up to first_ok cover the header
+    o, covered = 0, 0
+    while o < first_ok:
+        bs = struct.unpack_from("<H", raw, o + 16)[0] + 1
+        covered += struct.unpack_from("<I", raw, o + bs - 4)[0]
+        o += bs
+    assert o == first_ok and covered >= hsize > covered - 700
+    for world in (2, 3, 7, 40):
+        b = shard.member_boundaries(raw, world, hsize)
+        assert all(x >= first_ok for x in b[1:])
+        assert b == shard.member_boundaries(p, world, hsize)  # from windows of the file: the same cuts
