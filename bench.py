@@ -666,7 +666,9 @@ def run_uneven(args):
                    "form": "one CUDA graph per step: all scans, ONE inflate launch, all chains and columns",
                    "l2": "inputs larger than L2 (no flush)", "generate_s": round(gen_s, 1)},
         "records_per_s": n_rec / (ms / 1e3),
-        "autotune_inflate_ms": plan.tuning, "inflate_form": plan.form,
+        "autotune": {"params": plan.tuning["params"], "ms": plan.tuning["ms"], "seconds": plan.tuning["seconds"],
+                     "key": plan.tuning["key"]},
+        "inflate_form": plan.form,
         "stages_ms": {k: round(v, 3) for k, v in stage.items()},
         "one_launch_per_file": {"ms_per_step": ms_per_file, "value": inflated / (ms_per_file / 1e3) / 1e9,
                                 "records_per_s": n_rec / (ms_per_file / 1e3)},

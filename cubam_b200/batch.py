@@ -255,8 +255,9 @@ class BatchPlan:
     with one launch; :meth:`check` reads every device summary with one copy and raises on a
     status or on counts that differ from the plan.
 
-    ``form`` is the inflate form (1: a member per warp, 2: a member per lane); None lets
-    :meth:`autotune` time both on this batch and keep the faster.
+    ``form`` is the inflate form (1: a member per warp, 2: a member per lane, 3: decode per lane and
+    copy per warp); None lets :meth:`autotune` choose it, with the other launch parameters, by timing
+    this batch (or from the tuning cache for a batch of the same shape on the same device).
     """
 
     def __init__(self, files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "GN"), check_crc: bool = True,
@@ -408,25 +409,17 @@ class BatchPlan:
                     raise RuntimeError(f"file {k}: the record chain differs from the plan")
 
     # ------------------------------------------------------------------ tuning and graphs
-    def autotune(self, reps: int = 2) -> dict:
-        """Time the batch with each inflate form (1: a member per warp, 2: a member per lane, 3: decode per
-        lane and copy per warp) and keep the fastest; returns the inflate milliseconds per form."""
-        times = {}
-        for form in (1, 2, 3):
-            self.launch(form)
-            torch.cuda.synchronize()
-            self.check()
-            best = None
-            for _ in range(reps):
-                ev = StageEvents()
-                self.launch(form, ev)
-                torch.cuda.synchronize()
-                ms = ev.ms()["inflated"]
-                best = ms if best is None else min(best, ms)
-            times[form] = best
-        self.form = min(times, key=times.get)
-        self.tuning = times
-        return times
+    def autotune(self, reps: int = 2, cache_path=None, use_cache: bool = True) -> dict:
+        """Choose the launch parameters for this batch by timing it (:func:`cubam_b200.tune.tune`: the
+        inflate form 1-3, form 3's decoder roots, copy warps, decode steps and prefetch, the chain tile),
+        apply them to the process and cache them by device and batch shape; returns the tuner's entry
+        (``params`` and the milliseconds of every candidate)."""
+        from cubam_b200 import tune
+
+        entry = tune.tune(self, reps=reps, path=cache_path, use_cache=use_cache)
+        self.form = entry["params"]["inflate_form"]
+        self.tuning = entry
+        return entry
 
     def capture(self) -> None:
         """Record :meth:`launch` as a CUDA graph (after one eager run has set every kernel up)."""

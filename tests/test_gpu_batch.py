@@ -75,7 +75,7 @@ def test_batch_plan_forms_and_graph_replay(uneven):
     files = [(comp, hdr) for _, comp, hdr in uneven]
     ref = batch.decode_many(files, tags=TAGS)
     plan = batch.BatchPlan(files, tags=TAGS)
-    assert plan.form in (1, 2, 3) and set(plan.tuning) == {1, 2, 3}
+    assert plan.form in (1, 2, 3) and set(plan.tuning["ms"]["inflate_form"]) == {"1", "2", "3"}
     for form in (1, 2, 3):
         for r in plan.results:  # nothing stale can pass
             r.data.fill_(0)
