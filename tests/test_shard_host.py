@@ -21,6 +21,10 @@ from oracle import bam_oracle  # noqa: E402
 ROOT = Path(__file__).resolve().parents[1]
 
 
+#: the 28-byte BGZF end-of-file member (an empty member holding one fixed-Huffman final block)
+EOF_MEMBER = bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000")
+
+
 def _member(payload: bytes, level: int = 0) -> bytes:
     c = zlib.compressobj(level, zlib.DEFLATED, -15)
     body = c.compress(payload) + c.flush()
@@ -43,7 +47,7 @@ def test_boundaries_are_member_starts(name):
 def test_headers_inside_payloads_are_not_boundaries():
     fake = b"\x1f\x8b\x08\x04" + b"\0" * 6 + struct.pack("<H", 6) + b"BC" + struct.pack("<HH", 2, 99)
     members = [_member(fake * 50 + bytes([i]) * 300) for i in range(40)]  # stored: the fakes stay visible
-    raw = b"".join(members) + _member(b"")
+    raw = b"".join(members) + EOF_MEMBER
     starts, o = [], 0
     for m in members:
         starts.append(o)
@@ -105,7 +109,7 @@ def _big_header_bam(tmp_path, member_bytes=700, extra_refs=3000):
     blob = head + records
     members = [_member(blob[i : i + member_bytes], 6) for i in range(0, len(blob), member_bytes)]
     p = tmp_path / "bighead.bam"
-    p.write_bytes(b"".join(members) + _member(b""))
+    p.write_bytes(b"".join(members) + EOF_MEMBER)
     return p, len(head)
 
 
