@@ -56,6 +56,8 @@ def raise_status(status: int, what: str) -> None:
         return
     if status in _MESSAGES:
         raise ValueError(_MESSAGES[status])
+    if status == _lib.TIMEOUT:
+        raise TimeoutError(f"{what}: deadline passed before it was served")
     raise RuntimeError(f"{what} failed (status {status})")
 
 

@@ -155,6 +155,8 @@ class Request:
     m1: int = 0
     done: float | None = None
     result: DecodedFile | None = None
+    status: int = 0  # CB_OK, or CB_ERR_TIMEOUT when its deadline passed before it was served
+    error: Exception | None = None
     compressed_bytes: int = 0
     inflated_bytes: int = 0
     n_records: int = 0
@@ -164,6 +166,8 @@ class Request:
     _next: int = 0
     _last_launched: bool = False
     _off: torch.Tensor | None = None
+    _inflight: int = 0  # queued steps holding slices of it
+    _cancelled: bool = False
 
 
 def plan_request(rf: ResidentFile, req: Request) -> None:
@@ -343,12 +347,20 @@ class Server:
     ``step_bytes`` compressed bytes, or ``short_step_bytes`` while a request of at most
     ``small_bytes`` waits to start: shorter steps for a small request's latency, longer ones for
     throughput.
+
+    ``request_timeout`` (seconds after arrival, None for none) bounds how long a request may wait: when
+    it passes, a request not yet admitted or not yet started is dropped at once, and a started one gets
+    no further slices and gives its memory back once the steps already queued with it are done.  Either
+    way it finishes with ``status`` CB_ERR_TIMEOUT, ``error`` a TimeoutError and no result.
     """
 
     def __init__(self, files: list[ResidentFile], budget_bytes: int = 40 << 30, step_bytes: int = 320 << 20,
                  slice_bytes: int = 48 << 20, tags=("CB", "UB", "GN"), check_crc: bool = True,
-                 pool_frac: float = 0.7, short_step_bytes: int = 128 << 20, small_bytes: int = 8 << 20):
+                 pool_frac: float = 0.7, short_step_bytes: int = 128 << 20, small_bytes: int = 8 << 20,
+                 request_timeout: float | None = None):
         self.files = files
+        self.request_timeout = request_timeout
+        self.timed_out = 0
         self.tags = tuple(tags)
         self.check_crc = check_crc
         self.long_step_bytes = int(step_bytes)
@@ -404,7 +416,7 @@ class Server:
             ix = self.files[r.file].index
             return int(ix.coff[r.m1]) - (int(ix.coff[r._slices[r._next][0]]) if r._next < len(r._slices) else 0)
 
-        ready = [r for r in self.active if not r._last_launched]
+        ready = [r for r in self.active if not r._last_launched and not r._cancelled]
         if not ready:
             return []
         small_waiting = any(r.compressed_bytes <= self.small_bytes and r._next == 0 for r in ready) or any(
@@ -444,6 +456,8 @@ class Server:
         s = stream_ptr()
         scratch = self.scratch[self.steps % 2]  # the step before may still be read back by the host
         rows = []
+        for sl in slices:
+            sl.req._inflight += 1
         for sl in slices:
             r, rf = sl.req, self.files[sl.req.file]
             ix = rf.index
@@ -497,7 +511,7 @@ class Server:
         host[isz : isz + ncs].copy_(csumm[:ncs], non_blocking=True)
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
-        return ev, n_jobs, checks, done, host[:isz], host[isz : isz + ncs], ev0
+        return ev, n_jobs, checks, done, host[:isz], host[isz : isz + ncs], ev0, [sl.req for sl in slices]
 
     def _check(self, n_jobs, checks, summ, csumm) -> None:
         """Statuses of a completed step from its summaries in pinned host memory."""
@@ -515,11 +529,39 @@ class Server:
     def release(self, req: Request) -> None:
         """Give a finished request's device memory back (its result must no longer be used)."""
         if req._region >= 0:
-            self.alloc.release(req._region, max(req._region_size, 1))
-            req._region = -1
-            self.side_used -= req.n_records * record_bytes(len(self.tags))
+            self._free(req)
             req.result = None
-            req._off = None
+
+    def _expire(self, now: float, finish) -> None:
+        """Apply ``request_timeout`` at host time ``now`` (seconds since the loop's t0)."""
+        if self.request_timeout is None:
+            return
+        late = [r for r in self.pending if now - r.arrival > self.request_timeout]
+        for r in late:
+            self.pending.remove(r)
+            finish(r)
+        for r in [r for r in self.active if not r._cancelled and now - r.arrival > self.request_timeout]:
+            if r._last_launched:  # its last slice is queued: it is served
+                continue
+            r._cancelled = True
+            if r._inflight == 0:
+                self.active.remove(r)
+                self._free(r)
+                finish(r)
+
+    def _time_out(self, r: Request, now: float) -> None:
+        r.done = now
+        r.status = _lib.TIMEOUT
+        r.error = TimeoutError(f"request {r.rid} not served within {self.request_timeout} s of its arrival")
+        r.result = None
+        self.timed_out += 1
+
+    def _free(self, r: Request) -> None:
+        if r._region >= 0:
+            self.alloc.release(r._region, max(r._region_size, 1))
+            r._region = -1
+            self.side_used -= r.n_records * record_bytes(len(self.tags))
+            r._off = None
 
     # -------------------------------------------------------------- the loop
     def run(self, requests: list[Request], on_done=None, t0: float | None = None) -> list[Request]:
@@ -541,10 +583,18 @@ class Server:
                 self.submit(incoming[i])
                 i += 1
 
+        def timed_out(r):
+            self._time_out(r, time.perf_counter() - t0)
+            finished.append(r)
+            if on_done:
+                on_done(r)
+
         def complete(step):
-            ev, n_jobs, checks, done, summ, csumm = step
+            ev, n_jobs, checks, done, summ, csumm, _, touched = step
             now = time.perf_counter() - t0
             self._check(n_jobs, checks, summ, csumm)
+            for r in touched:
+                r._inflight -= 1
             for r in done:
                 r.done = now
                 self.active.remove(r)
@@ -552,11 +602,17 @@ class Server:
                 keep = on_done(r) if on_done else None
                 if keep is not False:
                     self.release(r)
+            for r in {id(r): r for r in touched}.values():  # cancelled: free once no queued step holds it
+                if r._cancelled and r._inflight == 0 and r in self.active:
+                    self.active.remove(r)
+                    self._free(r)
+                    timed_out(r)
 
         clock = time.perf_counter
         while i < len(incoming) or self.pending or self.active or inflight:
             ta = clock()
             arrivals()
+            self._expire(clock() - t0, timed_out)
             self._admit()
             launched = False
             if len(inflight) < 2:
@@ -577,7 +633,7 @@ class Server:
                     self.host_s["wait"] += td - tc
                     step = inflight.pop(0)
                     self.gpu_ms += step[6].elapsed_time(step[0])
-                    complete(step[:6])
+                    complete(step)
                     self.host_s["complete"] += clock() - td
                 else:
                     time.sleep(0.0002)

@@ -32,7 +32,8 @@ enum {
     CB_ERR_CAPACITY = 7,      /* an output or workspace buffer given by the caller is too small */
     CB_ERR_CUDA = 8,          /* a CUDA call failed (cb_last_error() has the text) */
     CB_ERR_ARG = 9,           /* invalid argument */
-    CB_ERR_TIMEOUT = 10       /* a bounded device-side wait ran out */
+    CB_ERR_TIMEOUT = 10       /* a serving request's deadline passed before it was served (no kernel of
+                                 this library waits on another, so no device wait returns it) */
 };
 
 /* One BGZF member to inflate: DEFLATE payload at `in` (in_len bytes), output

@@ -122,3 +122,32 @@ def test_served_in_a_mix_equals_alone(files):
         assert r.done is not None and r.done >= r.arrival
     lat = serve.latency_summary(done)
     assert lat["all_ms"]["n"] == len(reqs)
+
+
+def test_request_timeout(files):
+    """With a deadline of 0 s every request times out (those not started at once, those started after
+    their queued steps), the rest of the loop carries on, and all memory comes back; without one the
+    same requests are all served."""
+    rng = np.random.default_rng(9)
+    reqs = []
+    for f, rf in enumerate(files):
+        for a, b in _ranges(rf, rng, 6):
+            reqs.append(serve.Request(f, rf.voff(a), rf.voff(b), arrival=0.0, rid=len(reqs)))
+    seen = []
+    server = serve.Server(files, budget_bytes=48 << 20, step_bytes=1 << 20, slice_bytes=256 << 10, tags=TAGS,
+                          request_timeout=0.0)
+    done = server.run(reqs, on_done=seen.append)
+    assert len(done) == len(reqs) == len(seen)
+    late = [r for r in done if r.status == serve._lib.TIMEOUT]
+    assert late and server.timed_out == len(late)
+    for r in late:
+        assert r.result is None and isinstance(r.error, TimeoutError)
+    for r in done:
+        assert r.status in (0, serve._lib.TIMEOUT)
+    assert server.alloc.free == [(0, server.pool_bytes)] and server.side_used == 0 and not server.active
+
+    again = [serve.Request(r.file, r.voff_begin, r.voff_end, rid=r.rid) for r in reqs]
+    server = serve.Server(files, budget_bytes=48 << 20, step_bytes=1 << 20, slice_bytes=256 << 10, tags=TAGS,
+                          request_timeout=60.0)
+    done = server.run(again)
+    assert server.timed_out == 0 and all(r.status == 0 for r in done) and len(done) == len(again)

@@ -1,77 +1,70 @@
-"""Host logic of the serving loop (no GPU): the pool allocator, request slicing, Poisson requests."""
+"""Host logic of the serving loop's request deadline (no device work)."""
 
-import numpy as np
-import pytest
-
-pytest.importorskip("torch")
-
-from cubam_b200 import serve  # noqa: E402
+from cubam_b200 import _lib, serve
 
 
-def test_pool_allocator_first_fit_and_coalescing():
-    a = serve.PoolAllocator(4096)
-    x = a.alloc(1000)  # rounded to 1024
-    y = a.alloc(1)  # 256
-    z = a.alloc(2000)  # 2048
-    assert (x, y, z) == (0, 1024, 1280)
-    assert a.alloc(1024) is None and a.available() == 4096 - 1024 - 256 - 2048
-    a.release(y, 1)
-    assert a.alloc(200) == 1024  # first fit reuses the hole
-    a.release(1024, 200)
-    a.release(x, 1000)
-    a.release(z, 2000)
-    assert a.free == [(0, 4096)]
+def _server(timeout):
+    s = serve.Server.__new__(serve.Server)
+    s.request_timeout = timeout
+    s.timed_out = 0
+    s.tags = ("CB",)
+    s.alloc = serve.PoolAllocator(1 << 20)
+    s.side_used = 0
+    s.pending, s.active = [], []
+    return s
 
 
-class _FakeIndex:
-    def __init__(self, coff, first_rec):
-        self.coff = np.asarray(coff, np.int64)
-        self.first_rec = np.asarray(first_rec, np.int64)
-        self.ucum = np.arange(len(coff), dtype=np.int64) * 65280
-        self.cum_rec = np.arange(len(coff), dtype=np.int64) * 100
+def _admitted(s, rid, arrival, **kw):
+    r = serve.Request(0, 0, 0, arrival=arrival, rid=rid)
+    r._region_size, r.n_records = 4096, 10
+    r._region = s.alloc.alloc(4096)
+    s.side_used += r.n_records * serve.record_bytes(len(s.tags))
+    for k, v in kw.items():
+        setattr(r, k, v)
+    s.active.append(r)
+    return r
 
 
-class _FakeFile:
-    def __init__(self, coff, first_rec):
-        self.index = _FakeIndex(coff, first_rec)
+def test_deadline_rules():
+    s = _server(1.0)
+    waiting_late, waiting_new = serve.Request(0, 0, 0, arrival=0.0, rid=1), serve.Request(0, 0, 0, arrival=5.0, rid=2)
+    s.pending += [waiting_late, waiting_new]
+    idle = _admitted(s, 3, 0.0)  # admitted, nothing queued
+    running = _admitted(s, 4, 0.0, _next=1, _inflight=1)  # a step holding it is queued
+    last = _admitted(s, 5, 0.0, _last_launched=True, _inflight=1)  # its last slice is queued: served
+    fresh = _admitted(s, 6, 1.5)
+    out = []
 
-    boundaries = serve.ResidentFile.boundaries
-    voff = serve.ResidentFile.voff
-    member_of = serve.ResidentFile.member_of
+    def finish(r):
+        s._time_out(r, 2.0)
+        out.append(r)
 
-    @property
-    def n_members(self):
-        return len(self.index.coff) - 1
-
-
-def test_slices_cut_at_record_starts_within_the_limit():
-    # 10 members of 1000 compressed bytes; no record starts in members 3 and 7
-    coff = np.arange(11) * 1000
-    first = [5, 0, 12, -1, 40, 0, 3, -1, 8, 1, 0]
-    rf = _FakeFile(coff, first)
-    req = serve.Request(0, rf.voff(0), rf.voff(10))
-    req.m0, req.m1 = 0, 10
-    for limit, want in [
-        (2500, [(0, 2), (2, 4), (4, 6), (6, 8), (8, 10)]),
-        (1000, [(0, 1), (1, 2), (2, 4), (4, 5), (5, 6), (6, 8), (8, 9), (9, 10)]),
-        (100_000, [(0, 10)]),
-    ]:
-        assert serve.slice_request(rf, req, limit) == want
-    with pytest.raises(ValueError):
-        rf.member_of((3000 << 16) | 0)  # no record starts in member 3
-    with pytest.raises(ValueError):
-        rf.member_of((4000 << 16) | 41)  # not the first record of member 4
-    assert rf.member_of(rf.voff(4)) == 4
+    s._expire(2.0, finish)
+    assert [r.rid for r in out] == [1, 3]
+    assert s.pending == [waiting_new] and idle not in s.active and idle._region == -1
+    assert running._cancelled and running in s.active and running._region >= 0
+    assert not last._cancelled and not fresh._cancelled
+    for r in out:
+        assert r.status == _lib.TIMEOUT and isinstance(r.error, TimeoutError) and r.done == 2.0
+    assert s.timed_out == 2
+    # the running one is freed by the loop once its queued step completes; the rest hold memory
+    assert s.alloc.available() == (1 << 20) - 3 * 4096
 
 
-def test_poisson_requests_are_record_aligned_and_ordered():
-    coff = np.arange(201) * 30_000
-    first = np.where(np.arange(201) % 7 == 3, -1, 17)
-    first[-1] = 0
-    rf = _FakeFile(coff, first)
-    reqs = serve.poisson_requests([rf, rf], 300, rate=200.0, seed=1, min_bytes=64 << 10, max_bytes=4 << 20)
-    t = [r.arrival for r in reqs]
-    assert t == sorted(t) and 0.5 < t[-1] < 3.0  # ~1.5 s of arrivals at 200/s
-    for r in reqs:
-        m0, m1 = rf.member_of(r.voff_begin), rf.member_of(r.voff_end)
-        assert m0 < m1
+def test_no_deadline():
+    s = _server(None)
+    s.pending.append(serve.Request(0, 0, 0, arrival=0.0))
+    _admitted(s, 1, 0.0)
+    s._expire(1e9, lambda r: (_ for _ in ()).throw(AssertionError("nothing expires")))
+    assert len(s.pending) == 1 and len(s.active) == 1
+
+
+def test_timeout_status_raises_timeout_error():
+    import pytest
+
+    from cubam_b200.bgzf import raise_status
+
+    with pytest.raises(TimeoutError, match="deadline"):
+        raise_status(_lib.TIMEOUT, "request 3")
+    with pytest.raises(ValueError, match="Too many candidates"):
+        raise_status(_lib.TOO_MANY, "scan")
