@@ -48,8 +48,11 @@ sys.path.insert(0, str(ROOT))
 METRIC = "BAM decode GB/s (uncompressed) & records/s on 1 B200"
 UNIT = "GB/s"
 FALLBACK_HBM = 6650.0
+#: DRAM bytes (read + write) per inflated byte of each inflate form, from one ncu capture each on the
+#: 4M-record GEX file (1,008,824,685 inflated bytes); the bench scales them by its inflated bytes
 TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9,
-                    "k_inflate_warp": (1.593613e9 + 1.004537e9) / 1.008824685e9}
+                    "k_inflate_warp": (1.593613e9 + 1.004537e9) / 1.008824685e9,
+                    "k_decode + k_copy": (0.41414656e9 + 0.754893568e9 + 1.479409e9 + 0.955981568e9) / 1.008824685e9}
 
 
 def parse():
