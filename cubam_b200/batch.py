@@ -38,7 +38,17 @@ from cubam_b200.bgzf import (
 )
 
 #: kernels launched by each entry point (for the launch count of a step)
-KERNELS = {"scan": 4, "inflate": 3, "chain": 5, "decode": 1, "tags": 1}
+KERNELS = {"scan": 4, "inflate": 3, "chain": 9, "records": 1}
+
+
+def _tag_arrays(k: int, nrec: int):
+    """Tag-major type, value offset, value length and integer value arrays of k tags (device)."""
+    if not k:
+        return ()
+    return (torch.empty((k, nrec), dtype=torch.uint8, device="cuda"),
+            torch.empty((k, nrec), dtype=torch.int64, device="cuda"),
+            torch.empty((k, nrec), dtype=torch.int32, device="cuda"),
+            torch.empty((k, nrec), dtype=torch.int64, device="cuda"))
 
 
 def inflate_launches(form: int = 0, n_jobs: int | None = None) -> int:
@@ -198,30 +208,20 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
             cols["name_hash"] = torch.empty(nrec, dtype=torch.uint64, device="cuda")
         tag_cols = {}
         if nrec:
-            if derived:
-                rc = _lib.lib.cb_decode_records(data.data_ptr(), off.data_ptr(), nrec,
-                                                *(cols[k].data_ptr() for k in FIELDS),
-                                                cols["aligned_length"].data_ptr(), cols["name_hash"].data_ptr(),
-                                                stream_ptr())
-                _lib.check(rc, "cb_decode_records")
-            else:
-                rc = _lib.lib.cb_decode_fixed(data.data_ptr(), off.data_ptr(), nrec,
-                                              *(cols[k].data_ptr() for k in FIELDS), stream_ptr())
-                _lib.check(rc, "cb_decode_fixed")
-            if tags:
-                k = len(tags)
-                ty = torch.empty((k, nrec), dtype=torch.uint8, device="cuda")
-                vo = torch.empty((k, nrec), dtype=torch.int64, device="cuda")
-                vl = torch.empty((k, nrec), dtype=torch.int32, device="cuda")
-                iv = torch.empty((k, nrec), dtype=torch.int64, device="cuda")
-                rc = _lib.lib.cb_find_tags(data.data_ptr(), off.data_ptr(), nrec, "".join(tags).encode(), k,
-                                           ty.data_ptr(), vo.data_ptr(), vl.data_ptr(), iv.data_ptr(), stream_ptr())
-                _lib.check(rc, "cb_find_tags")
+            # columns, derived columns and tags in one record pass
+            k = len(tags)
+            arrs = _tag_arrays(k, nrec)
+            rc = _lib.lib.cb_decode_columns(
+                data.data_ptr(), off.data_ptr(), nrec, *(cols[f].data_ptr() for f in FIELDS),
+                cols["aligned_length"].data_ptr() if derived else None, cols["name_hash"].data_ptr() if derived else None,
+                "".join(tags).encode(), k, *((a.data_ptr() for a in arrs) if k else (None,) * 4), stream_ptr())
+            _lib.check(rc, "cb_decode_columns")
+            if k:
                 view = _View(data, off)
                 for q, t in enumerate(tags):
-                    tag_cols[t] = Tag._from_columns(view, t, ty[q], vo[q], vl[q], iv[q])
+                    tag_cols[t] = Tag._from_columns(view, t, *(a[q] for a in arrs))
             if counter is not None:
-                counter["launches"] = counter.get("launches", 0) + KERNELS["decode"] + (KERNELS["tags"] if tags else 0)
+                counter["launches"] = counter.get("launches", 0) + KERNELS["records"]
         results.append(DecodedFile(header, data, off, cols, tag_cols, int(info.n_members), int(info.total_out)))
     if events:
         events.mark("decoded")
@@ -320,10 +320,7 @@ class BatchPlan:
             arrs = None
             tag_cols = {}
             if k:
-                arrs = (torch.empty((k, nrec), dtype=torch.uint8, device=dev),
-                        torch.empty((k, nrec), dtype=torch.int64, device=dev),
-                        torch.empty((k, nrec), dtype=torch.int32, device=dev),
-                        torch.empty((k, nrec), dtype=torch.int64, device=dev))
+                arrs = _tag_arrays(k, nrec)
                 view = _View(data, o)
                 for q, t in enumerate(self.tags):
                     tag_cols[t] = Tag._from_columns(view, t, arrs[0][q], arrs[1][q], arrs[2][q], arrs[3][q])
@@ -374,14 +371,12 @@ class BatchPlan:
             if not nrec:
                 continue
             cols = res.columns
-            rc = _lib.lib.cb_decode_fixed(res.data.data_ptr(), res.offset.data_ptr(), nrec,
-                                          *(cols[f].data_ptr() for f in FIELDS), s)
-            _lib.check(rc, "cb_decode_fixed")
-            if arrs is not None:
-                rc = _lib.lib.cb_find_tags(res.data.data_ptr(), res.offset.data_ptr(), nrec,
-                                           "".join(self.tags).encode(), len(self.tags), *(a.data_ptr() for a in arrs),
-                                           s)
-                _lib.check(rc, "cb_find_tags")
+            k = len(self.tags) if arrs is not None else 0
+            rc = _lib.lib.cb_decode_columns(res.data.data_ptr(), res.offset.data_ptr(), nrec,
+                                            *(cols[f].data_ptr() for f in FIELDS), None, None,
+                                            "".join(self.tags).encode(), k,
+                                            *((a.data_ptr() for a in arrs) if k else (None,) * 4), s)
+            _lib.check(rc, "cb_decode_columns")
         if events:
             events.mark("decoded")
 
@@ -390,7 +385,7 @@ class BatchPlan:
         chains = sum(1 for d in self.data if int(d.numel()))
         decodes = sum(1 for n in self.n_records if n)
         return (KERNELS["scan"] * self.n_files + inflate_launches(self.form or 0, self.job_base[-1]) + KERNELS["chain"] * chains
-                + (KERNELS["decode"] + (KERNELS["tags"] if self.tags else 0)) * decodes)
+                + KERNELS["records"] * decodes)
 
     def check(self) -> None:
         """Raise on any device status of the last run, or counts that differ from the plan (one sync)."""

@@ -20,6 +20,61 @@ __device__ __forceinline__ uint32_t ld_u32(const uint8_t* b, long long o) {
     return (uint32_t)b[o] | ((uint32_t)b[o + 1] << 8) | ((uint32_t)b[o + 2] << 16) | ((uint32_t)b[o + 3] << 24);
 }
 
+// Bytes of device data read straight from global memory (the accessor form of ld_u16 / ld_u32).
+struct GlobalBytes {
+    const uint8_t* g;
+    __device__ __forceinline__ uint32_t u8(long long o) const { return g[o]; }
+    __device__ __forceinline__ uint32_t u16(long long o) const { return ld_u16(g, o); }
+    __device__ __forceinline__ uint32_t u32(long long o) const { return ld_u32(g, o); }
+};
+
+// Bytes of device data from a copy staged in shared memory where it covers them, else from global
+// memory.  s[0] holds data byte r0 and data + r0 is 16-byte aligned, so byte o sits in word
+// (o - r0) / 4 of the copy; [r0, hi) is staged, and the copy has at least 4 bytes after hi - r0
+// rounded up to 4 (word reads fetch the word after the one holding o).
+struct StagedBytes {
+    const uint8_t* g;
+    const uint8_t* s;
+    long long r0, hi;
+    __device__ __forceinline__ bool in(long long o, int sz) const { return o >= r0 && o + sz <= hi; }
+    __device__ __forceinline__ uint32_t u8(long long o) const { return in(o, 1) ? s[o - r0] : __ldg(g + o); }
+    __device__ __forceinline__ uint32_t u16(long long o) const {
+        return in(o, 2) ? (uint32_t)s[o - r0] | ((uint32_t)s[o - r0 + 1] << 8) : ld_u16(g, o);
+    }
+    __device__ __forceinline__ uint32_t u32(long long o) const {
+        if (in(o, 4)) {
+            const long long r = o - r0;
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(s + (r & ~3LL));
+            return __funnelshift_r(w[0], w[1], (unsigned)(r & 3) * 8);
+        }
+        return ld_u32(g, o);
+    }
+};
+
+// Copy the data bytes [lo, hi) to shared memory `st` with the warp's 16-byte loads (coalesced; the
+// first and last 16-byte blocks are read whole, which never leaves the pages holding the range);
+// returns the window start r0 (lo rounded down to a 16-byte address).  The caller syncs the warp.
+__device__ __forceinline__ long long stage_bytes(const uint8_t* b, long long lo, long long hi, uint4* st) {
+    const int lane = threadIdx.x & 31;
+    const long long r0 = lo - (long long)(reinterpret_cast<uintptr_t>(b + lo) & 15);
+    const long long nblk = hi > lo ? (hi - r0 + 15) >> 4 : 0;
+    const uint4* src = reinterpret_cast<const uint4*>(b + r0);
+    for (long long j0 = 0; j0 < nblk; j0 += 128) {
+        uint4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const long long j = j0 + u * 32 + lane;
+            if (j < nblk) v[u] = __ldg(src + j);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const long long j = j0 + u * 32 + lane;
+            if (j < nblk) st[j] = v[u];
+        }
+    }
+    return r0;
+}
+
 // Exclusive prefix sum over the 32 lanes of a warp.
 template <class T> __device__ __forceinline__ T warp_exclusive_scan(T v, T& total) {
     const int lane = threadIdx.x & 31;

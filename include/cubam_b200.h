@@ -89,8 +89,9 @@ int cb_device_sm_count(void);
  *      src/cubam/_memory.py:11-23) ---------------------------------------------------------------
  * One value per key for the whole process, read by every later launch; the package's autotuner
  * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
- *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk: a power of two, 2 KiB-4 MiB, or 0:
- *                          chosen from the data size, about one tile per resident thread, 2-32 KiB (0)
+ *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk (a warp stages one in shared
+ *                          memory): a power of two, 2-32 KiB, or 0: 8 KiB, less for chunks too small
+ *                          to give 32 tiles per SM (0)
  *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (3)
  *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 6, 7 or 8 (7)
  *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 with a 16 KiB window per
@@ -225,6 +226,18 @@ int cb_decode_records(const uint8_t* data, const int64_t* offsets, int64_t n, in
                       int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
                       int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, int32_t* aligned_length,
                       uint64_t* name_hash, void* stream);
+
+/* The record pass in one launch: the fixed columns (all eleven pointers, or ref == NULL for none),
+ * aligned_length and name_hash (each skipped when NULL) and k <= 16 aux tags (k = 0 for none; layout
+ * as cb_find_tags), from one read of each record's bytes.  A warp stages the bytes of 32 consecutive
+ * records in shared memory with coalesced loads and each lane parses one record; bytes outside the
+ * staged window are read from global memory, so any offsets are accepted.  cb_decode_fixed,
+ * cb_decode_records and cb_find_tags are this pass with the other outputs left out. */
+int cb_decode_columns(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
+                      int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
+                      int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, int32_t* aligned_length,
+                      uint64_t* name_hash, const char* names, int32_t k, uint8_t* type, int64_t* voff,
+                      int32_t* vlen, int64_t* value, void* stream);
 
 /* ---- Tags: replaces find_tag, one launch per tag (src/cubam/_kernels.py:334-388, src/cubam/bam.py:184-208).
  * One aux walk per record finds k tags (k <= 16); `names` (host) holds 2k characters.  Output is
