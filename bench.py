@@ -78,6 +78,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="gex: skip the bounded serving sub-object")
     ap.add_argument("--form", type=int, default=0,
                     help="inflate form for every batch size (1 warp per member, 2 lane per member, 3 split); "
                          "0: the library's choice")
@@ -376,6 +377,7 @@ def run_ours(args):
         plain = plain_per_chunk(comp, header, args.chunk_bytes or (256 << 20), tags)
 
     fused = fused_record_pass(comp, header) if rank == 0 else None
+    serving = serving_probe(path, value / world, tags) if rank == 0 and not args.no_serving else None
 
     e2e = None
     if not args.no_e2e:
@@ -441,6 +443,8 @@ def run_ours(args):
         line["plain_per_chunk"] = plain
     if fused:
         line["fused_record_pass"] = fused
+    if serving:
+        line["serving"] = serving
     if e2e:
         line["e2e"] = e2e
     if cpu:
@@ -452,6 +456,50 @@ def run_ours(args):
         import torch.distributed as td
 
         td.destroy_process_group()
+
+
+def serving_probe(path, batch_gbs: float, tags, n_requests: int = 100) -> dict:
+    """The serving loop on the bench file, bounded: the file resident once, 100 requests of log-uniform
+    64 KB-512 MB compressed ranges (seed 5), first all at once (the loop's saturation throughput),
+    then as a Poisson stream at 80% of it; latency percentiles (all requests, and those of at most
+    8 MB compressed) and throughput against the batched decode of the whole file."""
+    import torch
+
+    from cubam_b200 import serve
+
+    rf = serve.ResidentFile.load(path)
+    files = [rf]
+    server = serve.Server(files, budget_bytes=40 << 30, tags=tags)
+
+    def sink(r):
+        if r.result is not None and len(r.result):
+            r.result.columns["pos"].sum()
+
+    server.run(serve.poisson_requests(files, 8, 1e9, seed=6), on_done=sink)  # set every kernel up
+    torch.cuda.synchronize()
+
+    def served(rate):
+        reqs = serve.poisson_requests(files, n_requests, rate, seed=5)
+        t = time.perf_counter()
+        done = server.run(reqs, on_done=sink, t0=t)
+        torch.cuda.synchronize()
+        span = time.perf_counter() - t
+        return {"throughput_gbs": sum(r.inflated_bytes for r in done) / span / 1e9, "span_s": round(span, 4),
+                **serve.latency_summary(done)}, done
+
+    sat, done = served(1e9)
+    mean = sum(r.inflated_bytes for r in done) / len(done)
+    rate = 0.8 * sat["throughput_gbs"] * 1e9 / mean
+    live, done = served(rate)
+    out = {"requests": n_requests, "files": 1, "rate_per_s": round(rate, 2),
+           "sizes": "log-uniform 64 KB-512 MB compressed ranges of the bench file, seed 5",
+           "small": "at most 8 MB compressed", "saturation": sat, "served": live,
+           "served_vs_batch": live["throughput_gbs"] / batch_gbs,
+           "saturation_vs_batch": sat["throughput_gbs"] / batch_gbs,
+           "batch_gbs": batch_gbs}
+    del server, files, rf
+    torch.cuda.empty_cache()
+    return out
 
 
 def fused_record_pass(comp, header):

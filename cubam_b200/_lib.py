@@ -19,7 +19,7 @@ LIB_PATH = _build.LIB
 OK, TRUNCATED, NO_CHAIN, CORRUPT_BLOCK, INFLATE, CRC, TOO_MANY, CAPACITY, CUDA, ARG, TIMEOUT = range(11)
 #: launch parameters (cb_set_param / cb_get_param)
 (PARAM_CHAIN_TILE, PARAM_INFLATE_FORM, PARAM_DECODE_ROOT, PARAM_COPY_WARPS, PARAM_DECODE_STEPS, PARAM_DECODE_PREFETCH,
- PARAM_SPLIT_MIN_JOBS) = range(1, 8)
+ PARAM_SPLIT_MIN_JOBS, PARAM_COPY_UNITS) = range(1, 9)
 
 
 class MemberJob(ctypes.Structure):
@@ -104,6 +104,31 @@ _SIGNATURES = {
     "cb_crc32_spans": (c_int, [P, P, P, I64, P, P]),
     "cb_adler32_spans": (c_int, [P, P, P, I64, P, P]),
 }
+
+
+class BatchFile(ctypes.Structure):
+    """cb_batch_file: one file's results in a native batch (device pointers)."""
+
+    _fields_ = [
+        ("data", c_void_p), ("data_bytes", c_int64), ("offsets", c_void_p), ("n_records", c_int64),
+        ("n_members", c_int64), ("inflated_bytes", c_int64), ("header_bytes", c_int64), ("n_ref", c_int32),
+        ("k_tags", c_int32),
+        *((name, c_void_p) for name in ("ref", "pos", "end", "mapq", "flag", "nref", "npos", "tlen", "l_seq",
+                                        "clip_left", "clip_right", "tag_type", "tag_voff", "tag_vlen", "tag_value")),
+    ]
+
+
+_SIGNATURES.update({
+    "cb_batch_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_int64), c_int32, c_char_p, c_int32, c_int, P,
+                                ctypes.POINTER(c_void_p)]),
+    "cb_batch_run": (c_int, [P, P]),
+    "cb_batch_capture": (c_int, [P, P]),
+    "cb_batch_check": (c_int, [P, P]),
+    "cb_batch_file_info": (c_int, [P, c_int32, ctypes.POINTER(BatchFile)]),
+    "cb_batch_total_jobs": (c_int64, [P]),
+    "cb_batch_form": (c_int, [P]),
+    "cb_batch_destroy": (None, [P]),
+})
 
 
 def _load() -> ctypes.CDLL:

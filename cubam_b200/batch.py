@@ -434,3 +434,99 @@ class BatchPlan:
         else:
             self.launch()
         return self.results
+
+
+class _DeviceArray:
+    """Device memory owned by a native batch, seen by torch through ``__cuda_array_interface__``."""
+
+    def __init__(self, ptr, shape, typestr: str, owner):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr or 0), False),
+                                         "version": 3, "strides": None}
+        self.owner = owner  # the batch stays alive while a tensor views its memory
+
+
+_TYPESTR = {torch.int32: "<i4", torch.uint8: "|u1", torch.uint16: "<u2", torch.int64: "<i8"}
+
+
+class NativeBatch:
+    """The batched decode run by the library itself (``cb_batch_*`` in ``include/cubam_b200.h``): the
+    same launch sequence as :class:`BatchPlan` -- every file's member scan, ONE inflate for the members
+    of all files, every file's record chain and one record pass per file -- planned, owned and run in
+    C++, so that a host that is not Python reaches it through the C ABI.
+
+    ``files`` holds (compressed bytes on the device, header) pairs; :meth:`run` decodes them again
+    (the results are rewritten in place), :meth:`capture` records a run as a CUDA graph that later runs
+    replay, :meth:`check` synchronises and raises on any status or count that differs from the plan.
+    """
+
+    def __init__(self, files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "GN"), check_crc: bool = True):
+        import ctypes
+
+        self.files = files
+        self.tags = tuple(tags)
+        n = len(files)
+        ptrs = (ctypes.c_void_p * n)(*[c.data_ptr() if c.numel() else None for c, _ in files])
+        sizes = (ctypes.c_int64 * n)(*[int(c.numel()) for c, _ in files])
+        handle = ctypes.c_void_p()
+        rc = _lib.lib.cb_batch_create(ptrs, sizes, n, "".join(self.tags).encode(), len(self.tags), int(check_crc),
+                                      stream_ptr(), ctypes.byref(handle))
+        _raise(rc, "cb_batch_create")
+        self._h = handle
+        self.results = [self._file(k) for k in range(n)]
+
+    def _file(self, k: int) -> DecodedFile:
+        info = _lib.BatchFile()
+        _raise(_lib.lib.cb_batch_file_info(self._h, k, info), "cb_batch_file_info")
+        n, kt = int(info.n_records), int(info.k_tags)
+
+        def view(ptr, dtype, shape):
+            if not all(shape):
+                return torch.empty(shape, dtype=dtype, device="cuda")
+            return torch.as_tensor(_DeviceArray(ptr, shape, _TYPESTR[dtype], self), device="cuda")
+
+        data = view(info.data, torch.uint8, (int(info.data_bytes),))
+        off = view(info.offsets, torch.int64, (n,))
+        cols = {f: view(getattr(info, f), t, (n,)) for f, t in _TYPES.items()}
+        tag_cols = {}
+        if kt:
+            arrs = (view(info.tag_type, torch.uint8, (kt, n)), view(info.tag_voff, torch.int64, (kt, n)),
+                    view(info.tag_vlen, torch.int32, (kt, n)), view(info.tag_value, torch.int64, (kt, n)))
+            v = _View(data, off)
+            for q, t in enumerate(self.tags):
+                tag_cols[t] = Tag._from_columns(v, t, *(a[q] for a in arrs))
+        return DecodedFile(self.files[k][1], data, off, cols, tag_cols, int(info.n_members), int(info.inflated_bytes))
+
+    @property
+    def form(self) -> int:
+        return int(_lib.lib.cb_batch_form(self._h))
+
+    def run(self) -> None:
+        _raise(_lib.lib.cb_batch_run(self._h, stream_ptr()), "cb_batch_run")
+
+    def capture(self) -> None:
+        _raise(_lib.lib.cb_batch_capture(self._h, stream_ptr()), "cb_batch_capture")
+
+    def check(self) -> None:
+        _raise(_lib.lib.cb_batch_check(self._h, stream_ptr()), "cb_batch_check")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            torch.cuda.synchronize()
+            _lib.lib.cb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def _raise(rc: int, what: str) -> None:
+    """The reference's exception for a status code, NativeError for CUDA and argument errors."""
+    if rc in (_lib.OK, _lib.CUDA, _lib.ARG):
+        if rc == _lib.ARG:
+            raise _lib.NativeError(f"{what}: {_lib.lib.cb_last_error().decode()}")
+        _lib.check(rc, what)
+        return
+    raise_status(rc, what)

@@ -30,13 +30,14 @@ struct Param {
     int64_t lo, hi, def;
 };
 constexpr Param kParams[] = {
-    {CB_PARAM_CHAIN_TILE, 0, 1 << 22, 0},
+    {CB_PARAM_CHAIN_TILE, 0, 32768, 0},
     {CB_PARAM_INFLATE_FORM, 1, 3, 3},
     {CB_PARAM_DECODE_ROOT, 6, 8, 7},
     {CB_PARAM_COPY_WARPS, 2, 24, 12},
     {CB_PARAM_DECODE_STEPS, 1, 64, 16},
     {CB_PARAM_DECODE_PREFETCH, 0, 16, 4},
     {CB_PARAM_SPLIT_MIN_JOBS, 0, 1LL << 40, 30000},
+    {CB_PARAM_COPY_UNITS, 1, 2, 1},
 };
 constexpr int kNParams = sizeof(kParams) / sizeof(kParams[0]);
 std::atomic<int64_t> g_param[kNParams] = {};
@@ -67,7 +68,7 @@ extern "C" int cb_set_param(int key, int64_t value) {
     if (value < kParams[i].lo || value > kParams[i].hi)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
     if (key == CB_PARAM_CHAIN_TILE && value && (value < 2048 || (value & (value - 1))))
-        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two >= 2048");
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two from 2048 to 32768");
     if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6 && value != 12 && value != 24)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3, 6, 12 or 24");
     g_param[i].store(value, std::memory_order_relaxed);

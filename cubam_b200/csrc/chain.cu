@@ -4,27 +4,43 @@
 // cubam tests the record predicate (is_record, src/cubam/_kernels.py:250-278) at every byte offset and
 // keeps the chain from offset 0.  Only offsets on that chain matter: the result is the walk from 0 that
 // follows block_size while the predicate holds, which is O(records), not O(bytes).  It is walked in
-// parallel by tiles:
+// parallel by tiles of CB_PARAM_CHAIN_TILE bytes (by default 8 KB, less for small chunks):
 //
-//  1. k_walk: one thread per tile (CB_PARAM_CHAIN_TILE bytes; by default 2-32 KB from the data size) finds the tile's first offset that passes the predicate and
-//     walks the block_size links from it (each record checked with the full predicate) up to the first
-//     offset past the tile: first[t], count[t], exit[t], and whether the walk broke inside the tile.
+//  1. k_walk: one warp per tile.  The tile's bytes (and a little after it) are copied to shared
+//     memory with coalesced 16-byte loads; the lanes test 32 offsets at a time for the tile's first
+//     offset that passes the predicate; one lane follows the block_size links from it in shared
+//     memory up to the first offset past the tile; then the lanes test the predicate on those records
+//     in parallel.  Out: first[t], count[t] (up to the first record that fails), exit[t], whether the
+//     walk broke inside the tile, and the records' offsets in the tile (16-bit, relative to it).
 //  2. k_check: tile t's walk is the true chain when its first offset is where the previous non-empty
 //     tile's walk left (exit); a tile whose candidate is not on the chain (a spurious match of the
 //     predicate) makes the chunk take the serial path.  With none (the usual case, none were seen in
 //     hundreds of MB of BAM data), the chain is the union of the tile walks up to the first broken one.
-//  3. k_count_* : prefix sum of the tile counts (three kernels), then k_emit re-walks each tile to
-//     write its offsets; k_finish writes the summary (records, tail, errors).
+//  3. k_count_* : prefix sum of the tile counts (three kernels), then k_emit writes each tile's
+//     offsets from its relative ones (no second walk); k_finish writes the summary (records, tail,
+//     errors).
 //  4. k_serial: the chain walked by one thread, for chunks where the tile walks disagree.
+
+#include <atomic>
 
 #include "common.cuh"
 
 namespace cb {
 namespace chain {
 
-constexpr long long T_MIN = 2048;  // smallest tile (the workspace is sized for it)
+constexpr long long T_MIN = 2048;   // smallest tile
+constexpr long long T_MAX = 32768;  // largest tile (shared memory per warp)
 constexpr int NT = 256;
-constexpr int SCAN = 1024;         // tiles per block of the count scan
+constexpr int WW = 4;               // warps per block of k_walk
+constexpr int HALO = 512;           // bytes staged after the tile (headers of records that cross its end)
+constexpr int SCAN = 1024;          // tiles per block of the count scan
+constexpr int MIN_RECORD = 37;      // bytes of the shortest record the predicate accepts (block_size >= 33)
+
+// Record offsets one tile can hold (records are at least MIN_RECORD bytes apart).
+__host__ __device__ inline long long rel_cap(long long T) { return T / MIN_RECORD + 2; }
+// Shared memory of one k_walk warp: the staged bytes (plus slack for word reads), the relative offsets.
+__host__ __device__ inline long long stage_bytes_for(long long T) { return ((T + HALO + 32 + 15) / 16) * 16; }
+__host__ __device__ inline long long warp_smem(long long T) { return stage_bytes_for(T) + ((rel_cap(T) * 2 + 15) / 16) * 16; }
 
 struct Ws {
     int64_t* first;    // per tile
@@ -33,8 +49,10 @@ struct Ws {
     int64_t* base;     // exclusive prefix of the counts
     int64_t* bsum;     // per scan block
     int64_t* meta;     // [0] inconsistent tile (min) [1] first broken tile (min) [2] any candidate [3] total
+    uint16_t* rel;     // per tile: its records' offsets relative to the tile start, rel_cap(T) slots
     long long ntiles, nblocks;
     long long T;       // bytes per tile
+    long long rcap;    // rel_cap(T)
 };
 
 __host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -57,14 +75,28 @@ __host__ __device__ inline Ws carve(void* ws, long long n, long long T) {
     w.base = reinterpret_cast<int64_t*>(p);
     p += align256(w.ntiles * 8);
     w.bsum = reinterpret_cast<int64_t*>(p);
+    p += align256(w.nblocks * 8);
+    w.rcap = rel_cap(T);
+    w.rel = reinterpret_cast<uint16_t*>(p);
     return w;
 }
 
-__host__ inline size_t ws_bytes(long long n) {
-    long long ntiles = (n + T_MIN - 1) / T_MIN;
+__host__ inline size_t ws_bytes_for(long long n, long long T) {
+    long long ntiles = (n + T - 1) / T;
     if (ntiles < 1) ntiles = 1;
     long long nblocks = (ntiles + SCAN - 1) / SCAN;
-    return 256 + 3 * align256(ntiles * 8) + align256(ntiles * 4) + align256(nblocks * 8) + 256;
+    return 256 + 3 * align256(ntiles * 8) + align256(ntiles * 4) + align256(nblocks * 8) +
+           align256(ntiles * rel_cap(T) * 2) + 256;
+}
+
+// Workspace for any tile size: the largest over the allowed sizes.
+__host__ inline size_t ws_bytes(long long n) {
+    size_t m = 0;
+    for (long long T = T_MIN; T <= T_MAX; T *= 2) {
+        const size_t b = ws_bytes_for(n, T);
+        if (b > m) m = b;
+    }
+    return m;
 }
 
 __device__ __forceinline__ int reg2bin(int beg, int end) {
@@ -77,47 +109,41 @@ __device__ __forceinline__ int reg2bin(int beg, int end) {
     return 0;
 }
 
-// The reference's record predicate at offset o (src/cubam/_kernels.py:250-278).
-__device__ bool is_record(const uint8_t* b, long long n, long long o, int n_ref) {
+// The reference's record predicate at offset o (src/cubam/_kernels.py:250-278), on the bytes of
+// accessor A (GlobalBytes or StagedBytes).
+template <class A> __device__ bool is_record_at(const A& b, long long n, long long o, int n_ref) {
     if (o < 0 || o + 36 > n) return false;
-    const int bs = (int)ld_u32(b, o);
+    const int bs = (int)b.u32(o);
     if (bs < 33 || bs > (1 << 22) || o + 4 + (long long)bs > n) return false;
-    const int ref = (int)ld_u32(b, o + 4), pos = (int)ld_u32(b, o + 8);
-    const int nref = (int)ld_u32(b, o + 24), npos = (int)ld_u32(b, o + 28);
+    const int ref = (int)b.u32(o + 4), pos = (int)b.u32(o + 8);
+    const int nref = (int)b.u32(o + 24), npos = (int)b.u32(o + 28);
     if (ref < -1 || ref >= n_ref || pos < -1 || nref < -1 || nref >= n_ref || npos < -1) return false;
-    const uint32_t lrn = b[o + 12], ncig = ld_u16(b, o + 16), flag = ld_u16(b, o + 18), lseq = ld_u32(b, o + 20);
+    const uint32_t w12 = b.u32(o + 12), w16 = b.u32(o + 16), lseq = b.u32(o + 20);
+    const uint32_t lrn = w12 & 255, ncig = w16 & 0xffff, flag = w16 >> 16;
     if (lrn < 2 || flag >= 4096 || lseq > (1u << 22)) return false;
     if (32LL + lrn + 4LL * ncig + (lseq + 1) / 2 + lseq > (long long)bs) return false;
     const long long nm = o + 36;
-    if (b[nm + lrn - 1] != 0) return false;
+    if (b.u8(nm + lrn - 1) != 0) return false;
     for (uint32_t i = 0; i + 1 < lrn; i++) {
-        const uint8_t c = b[nm + i];
+        const uint32_t c = b.u8(nm + i);
         if (c < 33 || c > 126 || c == '@') return false;
     }
     const long long cg = nm + lrn;
     long long rlen = 0;
     for (uint32_t i = 0; i < ncig; i++) {
-        const uint32_t v = ld_u32(b, cg + 4LL * i), op = v & 15;
+        const uint32_t v = b.u32(cg + 4LL * i), op = v & 15;
         if (op > 8) return false;
         if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) rlen += v >> 4;
     }
     if (pos >= 0) {
         const int end = pos + (int)(rlen > 0 ? rlen : 1);
-        if (ld_u16(b, o + 14) != (uint32_t)reg2bin(pos, end)) return false;
+        if ((w12 >> 16) != (uint32_t)reg2bin(pos, end)) return false;
     }
     return true;
 }
 
-// First offset in [lo, hi) that passes the predicate, or -1.  block_size is read from aligned words
-// (a 64-bit window) so that most offsets are rejected without the full test.
-__device__ long long first_candidate(const uint8_t* b, long long n, long long lo, long long hi, int n_ref) {
-    for (long long o = lo; o < hi; o++) {
-        if (o + 4 > n) return -1;
-        const uint32_t bs = ld_u32(b, o);
-        if (bs - 33u > (1u << 22) - 33u) continue;
-        if (is_record(b, n, o, n_ref)) return o;
-    }
-    return -1;
+__device__ __forceinline__ bool is_record(const uint8_t* b, long long n, long long o, int n_ref) {
+    return is_record_at(GlobalBytes{b}, n, o, n_ref);
 }
 
 __global__ void k_init(Ws w) {
@@ -127,29 +153,75 @@ __global__ void k_init(Ws w) {
     w.meta[3] = 0;
 }
 
-__global__ void __launch_bounds__(NT) k_walk(const uint8_t* b, long long n, int n_ref, Ws w) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long ts = t * w.T, te = min(ts + w.T, n);
-        const long long c = first_candidate(b, n, ts, te, n_ref);
-        long long o = c;
+__global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b, long long n, int n_ref, Ws w) {
+    extern __shared__ uint4 walk_mem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long T = w.T, sb = stage_bytes_for(T);
+    uint4* st = walk_mem + (size_t)warp * (warp_smem(T) / 16);
+    uint16_t* rel = reinterpret_cast<uint16_t*>(reinterpret_cast<uint8_t*>(st) + sb);
+    for (long long t = (long long)blockIdx.x * WW + warp; t < w.ntiles; t += (long long)gridDim.x * WW) {
+        const long long ts = t * T, te = min(ts + T, n);
+        const long long hi = min(te + HALO, n);
+        const long long r0 = stage_bytes(b, ts, hi, st);
+        const StagedBytes d{b, reinterpret_cast<const uint8_t*>(st), r0, hi};
+        // the tile's first offset that passes the predicate, 32 offsets at a time
+        long long c = -1;
+        for (long long base = ts; base < te; base += 32) {
+            const long long o = base + lane;
+            bool ok = false;
+            if (o < te && o + 4 <= n) {
+                const uint32_t bs = d.u32(o);
+                if (bs - 33u <= (1u << 22) - 33u) ok = is_record_at(d, n, o, n_ref);
+            }
+            const unsigned m = __ballot_sync(FULL, ok);
+            if (m) {
+                c = base + __ffs(m) - 1;
+                break;
+            }
+        }
         int cnt = 0;
         bool broken = false;
+        long long exit = -1;
         if (c >= 0) {
-            atomicOr(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
-            while (o < te) {
-                if (!is_record(b, n, o, n_ref)) {
-                    broken = true;
+            // one lane follows the links; a link that cannot be a record ends the list (the predicate
+            // fails there below)
+            int m = 0;
+            long long o = c;
+            if (lane == 0) {
+                while (o < te) {
+                    rel[m++] = (uint16_t)(o - ts);
+                    const uint32_t bs = o + 4 <= n ? d.u32(o) : 0u;
+                    if (o + 36 > n || bs < 33 || bs > (1u << 22) || o + 4 + (long long)bs > n) break;
+                    o += 4 + (long long)bs;
+                }
+            }
+            m = __shfl_sync(FULL, m, 0);
+            o = __shfl_sync(FULL, o, 0);
+            __syncwarp();
+            // the predicate on the listed records, in parallel: the count ends at the first failure
+            int f = m;
+            for (int j0 = 0; j0 < m; j0 += 32) {
+                const int j = j0 + lane;
+                const bool ok = j >= m || is_record_at(d, n, ts + rel[j], n_ref);
+                const unsigned bad = __ballot_sync(FULL, !ok);
+                if (bad) {
+                    f = j0 + __ffs(bad) - 1;
                     break;
                 }
-                cnt++;
-                o += 4 + (long long)ld_u32(b, o);
             }
-            if (broken) atomicMin(reinterpret_cast<long long*>(&w.meta[1]), t);
+            cnt = f;
+            broken = f < m;
+            exit = broken ? ts + rel[f] : o;
+            for (int j = lane; j < cnt; j += 32) w.rel[t * w.rcap + j] = rel[j];
         }
-        w.first[t] = c;
-        w.exit[t] = c >= 0 ? o : -1;
-        w.count[t] = cnt | (broken ? (int)0x80000000 : 0);
+        if (lane == 0) {
+            if (c >= 0) atomicOr(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
+            if (broken) atomicMin(reinterpret_cast<long long*>(&w.meta[1]), t);
+            w.first[t] = c;
+            w.exit[t] = exit;
+            w.count[t] = cnt | (broken ? (int)0x80000000 : 0);
+        }
+        __syncwarp();
     }
 }
 
@@ -202,20 +274,19 @@ __global__ void __launch_bounds__(SCAN) k_count_add(Ws w) {
     if (t < w.ntiles) w.base[t] += w.bsum[blockIdx.x];
 }
 
-__global__ void __launch_bounds__(NT) k_emit(const uint8_t* b, long long n, Ws w, int64_t* out, long long cap) {
+// Each tile's offsets, from its relative ones, at its place in the chain (a warp per tile).
+__global__ void __launch_bounds__(NT) k_emit(Ws w, int64_t* out, long long cap) {
     if (w.meta[0] != INT64_MAX || w.meta[3] > cap) return;
     const long long end = w.meta[1];
     if (w.first[0] != 0) return;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < w.ntiles;
-         t += (long long)gridDim.x * blockDim.x) {
-        if (t > end) continue;
+    const int lane = threadIdx.x & 31;
+    for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < w.ntiles;
+         t += ((long long)gridDim.x * blockDim.x) >> 5) {
+        if (t > end) break;
         const int cnt = w.count[t] & 0x7fffffff;
-        long long o = w.first[t];
-        long long k = w.base[t];
-        for (int i = 0; i < cnt; i++) {
-            out[k + i] = o;
-            o += 4 + (long long)ld_u32(b, o);
-        }
+        const long long k = w.base[t], ts = t * w.T;
+        const uint16_t* r = w.rel + t * w.rcap;
+        for (int j = lane; j < cnt; j += 32) out[k + j] = ts + r[j];
     }
 }
 
@@ -314,26 +385,44 @@ extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, in
     if (workspace_bytes < chain::ws_bytes(n)) return CB_ERR_CAPACITY;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     long long tile = cb_param(CB_PARAM_CHAIN_TILE);
-    if (tile == 0) {
-        // about one walk per thread that the GPU keeps resident (1,024 per SM): big enough tiles for the
-        // first-candidate search to be rare, enough of them for the dependent loads to overlap
-        const long long want = n / ((long long)cb_device_sm_count() * 1024);
-        tile = chain::T_MIN;
-        while (tile < 32768 && tile * 2 <= want) tile *= 2;
-    }
-    chain::Ws w = chain::carve(workspace, n, tile);
     const long long sms = cb_device_sm_count();
+    if (tile == 0) {
+        // 8 KB tiles (a warp stages one, about 32 records), smaller ones for chunks too small to give
+        // 32 tiles per SM
+        tile = 8192;
+        while (tile > chain::T_MIN && n / tile < sms * 32) tile /= 2;
+    }
+    if (tile < chain::T_MIN || tile > chain::T_MAX || (tile & (tile - 1))) return CB_ERR_ARG;
+    chain::Ws w = chain::carve(workspace, n, tile);
+    const size_t smem = (size_t)chain::WW * chain::warp_smem(tile);
+    {
+        static std::atomic<bool> attr_set[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !attr_set[dev].load(std::memory_order_acquire)) {
+            const cudaError_t e = cudaFuncSetAttribute(chain::k_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)(chain::WW * chain::warp_smem(chain::T_MAX)));
+            if (e != cudaSuccess) return cb_set_error(e);
+            if (dev >= 0 && dev < 64) attr_set[dev].store(true, std::memory_order_release);
+        }
+    }
     long long grid = (w.ntiles + chain::NT - 1) / chain::NT;
     if (grid > sms * 16) grid = sms * 16;
     if (grid < 1) grid = 1;
+    long long wgrid = (w.ntiles + chain::WW - 1) / chain::WW;
+    if (wgrid > sms * 32) wgrid = sms * 32;
+    if (wgrid < 1) wgrid = 1;
+    long long egrid = (w.ntiles + chain::NT / 32 - 1) / (chain::NT / 32);
+    if (egrid > sms * 16) egrid = sms * 16;
+    if (egrid < 1) egrid = 1;
     chain::k_init<<<1, 1, 0, s>>>(w);
     if (n > 0) {
-        chain::k_walk<<<(unsigned)grid, chain::NT, 0, s>>>(data, n, n_ref, w);
+        chain::k_walk<<<(unsigned)wgrid, chain::WW * 32, smem, s>>>(data, n, n_ref, w);
         chain::k_check<<<(unsigned)grid, chain::NT, 0, s>>>(w);
         chain::k_count_blocks<<<(unsigned)w.nblocks, chain::SCAN, 0, s>>>(w);
         chain::k_count_top<<<1, chain::SCAN, 0, s>>>(w);
         chain::k_count_add<<<(unsigned)w.nblocks, chain::SCAN, 0, s>>>(w);
-        chain::k_emit<<<(unsigned)grid, chain::NT, 0, s>>>(data, n, w, offsets, cap);
+        chain::k_emit<<<(unsigned)egrid, chain::NT, 0, s>>>(w, offsets, cap);
         chain::k_serial<<<1, 1, 0, s>>>(data, n, n_ref, w, offsets, cap, summary);
     }
     chain::k_finish<<<1, 1, 0, s>>>(n, w, cap, summary);

@@ -51,27 +51,22 @@ struct StagedBytes {
     }
 };
 
-// Copy the data bytes [lo, hi) to shared memory `st` with the warp's 16-byte loads (coalesced; the
-// first and last 16-byte blocks are read whole, which never leaves the pages holding the range);
-// returns the window start r0 (lo rounded down to a 16-byte address).  The caller syncs the warp.
+// Copy the data bytes [lo, hi) to shared memory `st` with the warp's asynchronous 16-byte copies
+// (cp.async: coalesced, all in flight at once, no registers held; the first and last 16-byte blocks
+// are copied whole, which never leaves the pages holding the range), then wait for them and sync the
+// warp; returns the window start r0 (lo rounded down to a 16-byte address).
 __device__ __forceinline__ long long stage_bytes(const uint8_t* b, long long lo, long long hi, uint4* st) {
     const int lane = threadIdx.x & 31;
     const long long r0 = lo - (long long)(reinterpret_cast<uintptr_t>(b + lo) & 15);
     const long long nblk = hi > lo ? (hi - r0 + 15) >> 4 : 0;
     const uint4* src = reinterpret_cast<const uint4*>(b + r0);
-    for (long long j0 = 0; j0 < nblk; j0 += 128) {
-        uint4 v[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const long long j = j0 + u * 32 + lane;
-            if (j < nblk) v[u] = __ldg(src + j);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const long long j = j0 + u * 32 + lane;
-            if (j < nblk) st[j] = v[u];
-        }
+    for (long long j = lane; j < nblk; j += 32) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(st + j);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src + j) : "memory");
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
     return r0;
 }
 

@@ -670,9 +670,11 @@ static_assert(WIN == 32 * 32, "one 32-byte CRC column per lane");
 
 // WARPS_ warps per CTA, each with a ring of RING_ bytes: sources up to RING_ - 32 bytes back read
 // the ring, older ones the output already stored in HBM.
-template <int WARPS_, uint32_t RING_>
+template <int WARPS_, uint32_t RING_, int UPL_ = 1>
 struct CopyCfg {
     static constexpr int WARPS = WARPS_;
+    static constexpr int UPL = UPL_;              // units per lane in a group
+    static constexpr uint32_t GU = 32 * UPL_;     // units per group
     static constexpr uint32_t RING = RING_, RMASK = RING_ - 1;
     // a group's tokens start within GMAX bytes: its output (GMAX + 258 at most) and the unflushed
     // window before it (under WIN bytes) stay in the ring while the group is written
@@ -681,7 +683,7 @@ struct CopyCfg {
     struct CtaSmem {
         uint32_t crc8[8][256];
         uint32_t mulk[4][256];   // x * x^(8 (WIN - 32)) by bytes: moves a column past the other lanes
-        uint32_t tok[WARPS_][32];  // the tokens of the warp's current group, in order
+        uint32_t tok[WARPS_][32 * UPL_];  // the tokens of the warp's current group, in order
         alignas(16) uint8_t ring[WARPS_][RING_];
     };
 };
@@ -799,55 +801,110 @@ __global__ void __launch_bounds__(C::WARPS * 32)
         const uint32_t pad = (uint32_t)(-(int32_t)isize) & (WIN - 1);
         uint32_t p = 0, ws_ = 0, we = min((uint32_t)WIN - pad, isize), kwin = 0, col = 0;
         uint32_t st = (nu > isize) ? (uint32_t)CB_ERR_INFLATE : (uint32_t)CB_OK;
+        // groups of GU = 32 * UPL units, lane l holding units UPL * l ... UPL * l + UPL - 1 of the group
+        constexpr int UPL = C::UPL;
+        constexpr uint32_t GU = C::GU;
         uint32_t g = 0;
-        uint32_t u = ((uint32_t)lane < nu && st == CB_OK) ? (uint32_t)__ldcs(U + lane) : 0u;
+        uint32_t u[UPL];
+#pragma unroll
+        for (int h = 0; h < UPL; h++) {
+            const uint32_t i = UPL * lane + h;
+            u[h] = (i < nu && st == CB_OK) ? (uint32_t)__ldcs(U + i) : 0u;
+        }
         while (st == CB_OK && g < nu) {
-            // this group: units [g, g + cnt); a match head in lane 31 waits for the next group
-            const uint32_t avail = min(32u, nu - g);
-            const uint32_t nxt = __shfl_down_sync(FULL, u, 1);
-            const bool head31 = avail == 32 && (__shfl_sync(FULL, u, 31) & 0xC000u) == 0x8000u;
-            uint32_t cnt = avail - (head31 ? 1u : 0u);
-            const bool unit_head = (u & 0xC000u) == 0x8000u, unit_tail = (u & 0xC000u) == 0xC000u;
-            uint32_t len = (uint32_t)lane < cnt ? (!(u & 0x8000u) ? 1u : unit_head ? ((u >> 6) & 255u) + 3 : 0u) : 0u;
+            // this group: units [g, g + cnt); a match head as the group's last unit waits for the next group
+            const uint32_t avail = min(GU, nu - g);
+            const uint32_t nl = __shfl_down_sync(FULL, u[0], 1);  // the unit after this lane's last
+            const bool head_last = avail == GU && (__shfl_sync(FULL, u[UPL - 1], 31) & 0xC000u) == 0x8000u;
+            uint32_t cnt = avail - (head_last ? 1u : 0u);
+            uint32_t len[UPL], ex[UPL];
             uint32_t glen;
-            uint32_t ex = warp_exclusive_scan(len, glen);
+            auto lengths = [&](uint32_t c) {  // bytes of each unit's token, and where each starts
+                uint32_t tot = 0;
+#pragma unroll
+                for (int h = 0; h < UPL; h++) {
+                    const uint32_t x = u[h];
+                    len[h] = UPL * lane + h < c ? (!(x & 0x8000u) ? 1u : (x & 0xC000u) == 0x8000u ? ((x >> 6) & 255u) + 3 : 0u)
+                                                : 0u;
+                    tot += len[h];
+                }
+                uint32_t e0 = warp_exclusive_scan(tot, glen);
+#pragma unroll
+                for (int h = 0; h < UPL; h++) {
+                    ex[h] = e0;
+                    e0 += len[h];
+                }
+            };
+            lengths(cnt);
             if (glen > C::GMAX) {
-                // keep the units whose token starts within GMAX bytes (a tail goes with its head)
-                const uint32_t ex_prev = __shfl_up_sync(FULL, ex, 1);
-                const uint32_t start = (unit_tail && lane > 0) ? ex_prev : ex;
-                cnt = __popc(__ballot_sync(FULL, (uint32_t)lane < cnt && start < C::GMAX));
-                if ((uint32_t)lane >= cnt) len = 0;
-                ex = warp_exclusive_scan(len, glen);
+                // keep the units whose token starts within GMAX bytes (a tail goes with its head); the
+                // starts only grow along the units, so the kept units are a prefix
+                const uint32_t prev_ex = __shfl_up_sync(FULL, ex[UPL - 1], 1);
+                uint32_t kept = 0;
+#pragma unroll
+                for (int h = 0; h < UPL; h++) {
+                    const bool tail = (u[h] & 0xC000u) == 0xC000u;
+                    const uint32_t start = tail ? (h > 0 ? ex[h > 0 ? h - 1 : 0] : (lane > 0 ? prev_ex : ex[h])) : ex[h];
+                    kept += __popc(__ballot_sync(FULL, UPL * lane + h < cnt && start < C::GMAX));
+                }
+                cnt = kept;
+                lengths(cnt);
             }
-            const bool valid = (uint32_t)lane < cnt;
-            const bool is_head = valid && unit_head;
-            // a head's tail is the next unit of the group (a head at the end of the units is an error)
-            const bool bad_head = is_head && ((uint32_t)lane + 1 >= cnt || (nxt & 0xC000u) != 0xC000u);
-            const uint32_t dist = is_head ? ((((u & 63u) << 9) | (nxt & 511u)) + 1) : 0u;
+            // match heads: the distance from the head and its tail (the next unit; a head that is the
+            // last of the units, or not followed by a tail, is an error)
+            bool bad = false;
+            uint32_t tokv[UPL], myr[UPL], mybit[UPL];
+            bool is_tok[UPL];
+#pragma unroll
+            for (int h = 0; h < UPL; h++) {
+                const uint32_t i = UPL * lane + h;
+                const uint32_t x = u[h];
+                const uint32_t nx = h + 1 < UPL ? u[h + 1 < UPL ? h + 1 : 0] : nl;
+                const bool head = i < cnt && (x & 0xC000u) == 0x8000u;
+                const uint32_t dist = head ? ((((x & 63u) << 9) | (nx & 511u)) + 1) : 0u;
+                bad |= (head && (i + 1 >= cnt || (nx & 0xC000u) != 0xC000u)) || (head && dist > p + ex[h]);
+                is_tok[h] = len[h] != 0;
+                tokv[h] = head ? (0x80000000u | dist) : (x & 255u);
+                // a token starts in round ex >> 5 of the group, at bit ex & 31 of that round's start mask
+                myr[h] = is_tok[h] ? ex[h] >> 5 : 0xFFFFFFFFu;
+                mybit[h] = 1u << (ex[h] & 31u);
+            }
             // the next group's units are loaded while this one is written
             const uint32_t g2 = g + cnt;
-            const uint32_t u2 = (g2 + lane < nu) ? (uint32_t)__ldcs(U + g2 + lane) : 0u;
-            if (__any_sync(FULL, bad_head || (is_head && dist > p + ex)) || glen > isize - p) {
+            uint32_t u2[UPL];
+#pragma unroll
+            for (int h = 0; h < UPL; h++) {
+                const uint32_t i = g2 + UPL * lane + h;
+                u2[h] = i < nu ? (uint32_t)__ldcs(U + i) : 0u;
+            }
+            if (__any_sync(FULL, bad) || glen > isize - p) {
                 st = CB_ERR_INFLATE;
                 break;
             }
             // the group's tokens in order (tails are not tokens): literal byte, or 0x80000000 | distance
-            const bool is_tok = len != 0;
-            const unsigned tokmask = __ballot_sync(FULL, is_tok);
-            if (is_tok) tokw[__popc(tokmask & ((1u << lane) - 1u))] = is_head ? (0x80000000u | dist) : (u & 255u);
+            {
+                uint32_t ord = 0;
+                const uint32_t lower = (1u << lane) - 1u;
+#pragma unroll
+                for (int h = 0; h < UPL; h++) ord += __popc(__ballot_sync(FULL, is_tok[h]) & lower);
+#pragma unroll
+                for (int h = 0; h < UPL; h++)
+                    if (is_tok[h]) tokw[ord++] = tokv[h];
+            }
             __syncwarp();
-            // a token starts in round ex >> 5 of the group, at bit ex & 31 of that round's start mask
-            const uint32_t my_round = is_tok ? ex >> 5 : 0xFFFFFFFFu, my_bit = 1u << (ex & 31u);
             uint32_t before = 0;  // tokens that start before this round
             uint32_t ri = 0;
             for (uint32_t r0 = 0; r0 < glen; r0 += 32, ri++) {
                 const uint32_t rel = r0 + lane;
                 // the token of byte rel: tokens starting in this round set bits of a mask; the byte's
                 // token is the last one starting at or before it
-                const uint32_t sm = __reduce_or_sync(FULL, my_round == ri ? my_bit : 0u);
+                uint32_t mine = 0;
+#pragma unroll
+                for (int h = 0; h < UPL; h++) mine |= myr[h] == ri ? mybit[h] : 0u;
+                const uint32_t sm = __reduce_or_sync(FULL, mine);
                 const uint32_t ord = before + __popc(sm & incl) - 1;
                 before += __popc(sm);
-                const uint32_t t = tokw[ord & 31u];
+                const uint32_t t = tokw[ord & (GU - 1)];
                 const uint32_t b = p + rel;
                 uint32_t val = t & 255u;
                 int src = lane;  // the lane of this round holding the byte's source
@@ -883,7 +940,8 @@ __global__ void __launch_bounds__(C::WARPS * 32)
                 kwin++;
             }
             g = g2;
-            u = u2;
+#pragma unroll
+            for (int h = 0; h < UPL; h++) u[h] = u2[h];
         }
         if (st == CB_OK && p != isize) st = CB_ERR_INFLATE;
         if (st == CB_OK && crc && finish_crc(col, isize) != job.crc) st = CB_ERR_CRC;
@@ -991,21 +1049,20 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
             rc = launch_decode<split::DecCfg<6, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
         if (rc != CB_OK) return rc;
         const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
+        const bool two = cb_param(CB_PARAM_COPY_UNITS) == 2;
+#define CB_COPY(W, R, UPL) \
+    launch_copy<split::CopyCfg<W, R, UPL>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s)
         if (cw == 2)
-            rc = launch_copy<split::CopyCfg<2, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
-                                                      ws, s);
+            rc = CB_COPY(2, 16384, 1);
         else if (cw == 3)
-            rc = launch_copy<split::CopyCfg<3, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
-                                                      ws, s);
+            rc = CB_COPY(3, 16384, 1);
         else if (cw == 12)
-            rc = launch_copy<split::CopyCfg<12, 8192>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
-                                                      ws, s);
+            rc = two ? CB_COPY(12, 8192, 2) : CB_COPY(12, 8192, 1);
         else if (cw == 24)
-            rc = launch_copy<split::CopyCfg<24, 4096>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
-                                                      ws, s);
+            rc = two ? CB_COPY(24, 4096, 2) : CB_COPY(24, 4096, 1);
         else
-            rc = launch_copy<split::CopyCfg<6, 16384>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary,
-                                                      ws, s);
+            rc = two ? CB_COPY(6, 16384, 2) : CB_COPY(6, 16384, 1);
+#undef CB_COPY
         if (rc != CB_OK) return rc;
     }
     split::k_split_finish<<<1, 1, 0, s>>>(summary);

@@ -218,7 +218,6 @@ __global__ void __launch_bounds__(RW * 32) k_records(const uint8_t* __restrict__
         if (hi > lo + STAGE - 32) hi = lo + STAGE - 32;
         if (hi < lo) hi = lo;
         const long long r0 = stage_bytes(b, lo, hi, st);
-        __syncwarp();
         if (valid) {
             const Win w{b, reinterpret_cast<const uint8_t*>(st), r0, hi};
             parse_record(w, o, i, c, cols != 0, tag_code, k, t);

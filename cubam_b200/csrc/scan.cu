@@ -2,10 +2,11 @@
 // _inflate_blocks (src/cubam/_kernels.py:69-89, src/cubam/_kernels.py:662-702,
 // src/cubam/bgzf.py:542-586).
 //
-//  1. k_scan_count: each thread loads 16 bytes with one 128-bit load; __vcmpeq4 finds 0x1f bytes
-//     (about 1 in 256 in compressed data) and only those offsets get the full header test.  The
-//     count of every 4 KB tile goes to the workspace.
-//  2. k_scan_tiles: one block turns the tile counts into tile offsets (prefix sum).
+//  1. k_scan_count: a warp per 4 KB tile; each lane loads its eight 16-byte chunks with 128-bit
+//     loads, then __vcmpeq4 finds 0x1f bytes (about 1 in 256 in compressed data) and only those
+//     offsets get the full header test.  The count of every tile goes to the workspace.
+//  2. k_scan_tiles: one block turns the tile counts into tile offsets (prefix sum; each thread
+//     sums a contiguous run of tiles).
 //  3. k_scan_write: tiles with candidates are tested again and their offsets written in order
 //     (block prefix sum of the per-thread counts); no sort is needed.
 //  4. k_scan_finish: one block keeps the chain from offset 0 (all candidates in the usual case,
@@ -75,74 +76,86 @@ __device__ __forceinline__ bool member_at(const uint8_t* b, long long n, long lo
     return bs >= 26 && o + bs <= n;
 }
 
-// Bit mask (bit k = offset start + k) of the candidates in 16-byte chunk c of the aligned view of buf.
-__device__ __forceinline__ uint32_t chunk_candidates(const uint8_t* buf, long long n, long long c) {
-    uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
-    uintptr_t a = base + 16 * (uintptr_t)c;
-    long long start = (long long)(a - (uintptr_t)buf);
-    if (start >= n || start + 16 <= 0) return 0;
-    uint32_t w[4];
-    if (start >= 0 && start + 16 <= n) {
-        uint4 v = __ldg(reinterpret_cast<const uint4*>(a));
-        w[0] = v.x;
-        w[1] = v.y;
-        w[2] = v.z;
-        w[3] = v.w;
-    } else {
+// The 16 bytes of chunk c of the aligned view of buf (bytes outside [0, n) read as 0), and the
+// offset of its first byte.
+__device__ __forceinline__ uint4 chunk_load(const uint8_t* buf, long long n, long long c, long long& start) {
+    const uintptr_t base = (uintptr_t)buf & ~(uintptr_t)15;
+    const uintptr_t a = base + 16 * (uintptr_t)c;
+    start = (long long)(a - (uintptr_t)buf);
+    if (start >= 0 && start + 16 <= n) return __ldg(reinterpret_cast<const uint4*>(a));
+    uint32_t w[4] = {0, 0, 0, 0};
+    if (start < n && start + 16 > 0) {
         for (int k = 0; k < 4; k++) {
             uint32_t x = 0;
             for (int t = 0; t < 4; t++) {
-                long long o = start + 4 * k + t;
+                const long long o = start + 4 * k + t;
                 if (o >= 0 && o < n) x |= (uint32_t)buf[o] << (8 * t);
             }
             w[k] = x;
         }
     }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Bit mask (bit k = offset start + k) of the members that start in a chunk: __vcmpeq4 finds the
+// 0x1f bytes, and only those get the full header test.
+__device__ __forceinline__ uint32_t chunk_mask(const uint8_t* buf, long long n, long long start, uint4 v) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
     uint32_t mask = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         uint32_t eq = __vcmpeq4(w[k], 0x1f1f1f1fu);
         while (eq) {
-            int t = (__ffs(eq) - 1) >> 3;
+            const int t = (__ffs(eq) - 1) >> 3;
             eq &= ~(0xffu << (8 * t));
-            long long o = start + 4 * k + t;
+            const long long o = start + 4 * k + t;
             if (member_at(buf, n, o)) mask |= 1u << (4 * k + t);
         }
     }
     return mask;
 }
 
+__device__ __forceinline__ uint32_t chunk_candidates(const uint8_t* buf, long long n, long long c) {
+    long long start;
+    const uint4 v = chunk_load(buf, n, c, start);
+    return chunk_mask(buf, n, start, v);
+}
+
+// A warp per tile (NT chunks): each lane loads its NT / 32 chunks first, then tests them.
 __global__ void __launch_bounds__(NT) k_scan_count(const uint8_t* buf, long long n, Ws w) {
-    __shared__ uint32_t red[NT / 32];
-    for (long long t = blockIdx.x; t < w.ntiles; t += gridDim.x) {
-        uint32_t c = __popc(chunk_candidates(buf, n, t * NT + threadIdx.x));
-        for (int d = 16; d; d >>= 1) c += __shfl_down_sync(FULL, c, d);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t s = 0;
-            for (int i = 0; i < NT / 32; i++) s += red[i];
-            w.tile_count[t] = s;
-        }
-        __syncthreads();
+    constexpr int PER = NT / 32;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (NT / 32);
+    for (long long t = (long long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5); t < w.ntiles; t += nwarps) {
+        uint4 v[PER];
+        long long start[PER];
+#pragma unroll
+        for (int k = 0; k < PER; k++) v[k] = chunk_load(buf, n, t * NT + k * 32 + lane, start[k]);
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) c += __popc(chunk_mask(buf, n, start[k], v[k]));
+        c = __reduce_add_sync(FULL, c);
+        if (lane == 0) w.tile_count[t] = c;
     }
 }
 
-// Exclusive prefix sum of the tile counts (one block); meta[0] = total, meta[1] = status.
+// Exclusive prefix sum of the tile counts (one block, each thread a contiguous run of tiles);
+// meta[0] = total, meta[1] = status.
 __global__ void __launch_bounds__(FIN_NT) k_scan_tiles(Ws w, long long too_many) {
     __shared__ int64_t sm[33];
-    int64_t carry = 0;
-    for (long long b = 0; b < w.ntiles; b += FIN_NT) {
-        long long i = b + threadIdx.x;
-        int64_t v = i < w.ntiles ? (int64_t)w.tile_count[i] : 0;
-        int64_t tot;
-        int64_t x = block_exclusive_scan<FIN_NT>(v, tot, sm);
-        if (i < w.ntiles) w.tile_off[i] = carry + x;
-        carry += tot;
+    const long long per = (w.ntiles + FIN_NT - 1) / FIN_NT;
+    const long long a = min((long long)threadIdx.x * per, w.ntiles), b = min(a + per, w.ntiles);
+    int64_t sum = 0;
+    for (long long i = a; i < b; i++) sum += w.tile_count[i];
+    int64_t tot;
+    int64_t x = block_exclusive_scan<FIN_NT>(sum, tot, sm);
+    for (long long i = a; i < b; i++) {
+        w.tile_off[i] = x;
+        x += w.tile_count[i];
     }
     if (threadIdx.x == 0) {
-        w.meta[0] = carry;
-        w.meta[1] = carry > too_many ? CB_ERR_TOO_MANY : (carry > w.cap ? CB_ERR_CAPACITY : CB_OK);
+        w.meta[0] = tot;
+        w.meta[1] = tot > too_many ? CB_ERR_TOO_MANY : (tot > w.cap ? CB_ERR_CAPACITY : CB_OK);
     }
 }
 
@@ -227,11 +240,19 @@ __global__ void __launch_bounds__(FIN_NT) k_scan_finish(const uint8_t* buf, long
         __syncthreads();
     }
     const bool all = s_breaks == 0;
-    // last kept member -> used
-    for (long long i = tid; i < m; i += FIN_NT)
-        if (all || w.keep[i]) atomicMax(reinterpret_cast<unsigned long long*>(&s_last), (unsigned long long)i);
-    __syncthreads();
-    const long long last = s_last;
+    // last kept member -> used (every candidate is kept on the fast path)
+    if (!all) {
+        long long mine = -1;
+        for (long long i = tid; i < m; i += FIN_NT)
+            if (w.keep[i]) mine = i;
+        for (int d = 16; d; d >>= 1) {
+            const long long y = __shfl_down_sync(FULL, mine, d);
+            if (y > mine) mine = y;
+        }
+        if ((tid & 31) == 0 && mine > 0) atomicMax(reinterpret_cast<unsigned long long*>(&s_last), (unsigned long long)mine);
+        __syncthreads();
+    }
+    const long long last = all ? m - 1 : s_last;
     const long long used = w.cand[last] + (long long)ld_u16(buf, w.cand[last] + 16) + 1;
     if (eof && used != n) {
         if (tid == 0) summary->status = CB_ERR_TRUNCATED;
@@ -305,7 +326,10 @@ extern "C" int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t o
     int sms = cb_device_sm_count();
     long long grid = w.ntiles < (long long)sms * 8 ? w.ntiles : (long long)sms * 8;
     if (grid < 1) grid = 1;
-    scan::k_scan_count<<<(unsigned)grid, scan::NT, 0, s>>>(buf, n, w);
+    long long cgrid = (w.ntiles + scan::NT / 32 - 1) / (scan::NT / 32);
+    if (cgrid > (long long)sms * 16) cgrid = (long long)sms * 16;
+    if (cgrid < 1) cgrid = 1;
+    scan::k_scan_count<<<(unsigned)cgrid, scan::NT, 0, s>>>(buf, n, w);
     scan::k_scan_tiles<<<1, scan::FIN_NT, 0, s>>>(w, scan::cand_cap(n));
     scan::k_scan_write<<<(unsigned)grid, scan::NT, 0, s>>>(buf, n, w);
     scan::k_scan_finish<<<1, scan::FIN_NT, 0, s>>>(buf, n, eof, out_base_off, jobs, cap, summary, w);

@@ -3,7 +3,7 @@
 cubam launches its kernels with fixed shapes (``src/cubam/_kernels.py:637-641``) and reads with a
 fixed chunk policy (``src/cubam/_memory.py:11-23``).  Here the shapes that matter are launch
 parameters of the library (``cb_set_param``): the inflate form, the root bits of form 3's lane
-decoder, the warps and window of form 3's copy kernel, the decode steps between lane scheduling
+decoder, the warps, window and group size of form 3's copy kernel, the decode steps between lane scheduling
 rounds, the input prefetch distance, and the tile of the record chain's walk.  :func:`tune` times
 candidates on a real batch (a :class:`~cubam_b200.batch.BatchPlan`), one parameter at a time in the
 order of their effect (coordinate descent from the current values), keeps the fastest, applies it
@@ -33,14 +33,15 @@ CANDIDATES = {
     "inflate_form": (_lib.PARAM_INFLATE_FORM, (1, 2, 3)),
     "decode_root": (_lib.PARAM_DECODE_ROOT, (6, 7, 8)),
     "copy_warps": (_lib.PARAM_COPY_WARPS, (6, 12, 24)),
+    "copy_units": (_lib.PARAM_COPY_UNITS, (1, 2)),
     "decode_steps": (_lib.PARAM_DECODE_STEPS, (8, 16, 32)),
     "decode_prefetch": (_lib.PARAM_DECODE_PREFETCH, (0, 4, 8)),
-    "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 4096, 16384, 32768)),
+    "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 4096, 16384)),
 }
 #: the stage each parameter is timed on (StageEvents names)
 STAGE = {"chain_tile": "chained"}
 #: form-3 parameters are tuned only when form 3 wins
-FORM3 = ("decode_root", "copy_warps", "decode_steps", "decode_prefetch")
+FORM3 = ("decode_root", "copy_warps", "copy_units", "decode_steps", "decode_prefetch")
 
 
 def cache_path() -> Path:

@@ -102,6 +102,8 @@ int cb_device_sm_count(void);
  *   CB_PARAM_SPLIT_MIN_JOBS   with CB_PARAM_INFLATE_FORM 3, form 0 runs form 1 for calls of fewer jobs
  *                          (form 3 decodes one member per lane, so it needs many members to fill the GPU):
  *                          0 or more (30000)
+ *   CB_PARAM_COPY_UNITS    DEFLATE units each lane of form 3's copy kernel takes per group: 1 (groups of
+ *                          32 units) or 2 (groups of 64, with 6, 12 or 24 copy warps) (1)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
@@ -111,7 +113,8 @@ enum {
     CB_PARAM_COPY_WARPS = 4,
     CB_PARAM_DECODE_STEPS = 5,
     CB_PARAM_DECODE_PREFETCH = 6,
-    CB_PARAM_SPLIT_MIN_JOBS = 7
+    CB_PARAM_SPLIT_MIN_JOBS = 7,
+    CB_PARAM_COPY_UNITS = 8
 };
 int cb_set_param(int key, int64_t value);
 int64_t cb_get_param(int key);
@@ -310,6 +313,56 @@ int cb_crc32_spans(const uint8_t* data, const int64_t* off, const int64_t* size,
 /* zlib Adler-32 of each span (adler32_spans, src/cubam/_kernels.py:143-158). */
 int cb_adler32_spans(const uint8_t* data, const int64_t* off, const int64_t* size, int64_t n, uint32_t* out,
                      void* stream);
+
+/* ---- Batches: a fixed set of device-resident BAM files decoded by one launch sequence, recordable
+ * as one CUDA graph.  cubam decodes a chunk at a time with a host synchronisation per chunk
+ * (src/cubam/bgzf.py:625-652, src/cubam/bam.py:421-446); a batch's run issues every file's member
+ * scan (jobs into one table), ONE inflate for the members of all files, every file's record chain
+ * and every file's record pass (cb_decode_columns), with no host synchronisation. ---------------- */
+
+typedef struct cb_batch cb_batch;  /* opaque */
+
+/* One file's results (device pointers, valid until cb_batch_destroy; rewritten by every run). */
+typedef struct cb_batch_file {
+    const uint8_t* data;      /* the records: inflated bytes after the BAM header */
+    int64_t data_bytes;
+    const int64_t* offsets;   /* n_records record offsets into data */
+    int64_t n_records;
+    int64_t n_members;        /* BGZF members, empty ones included */
+    int64_t inflated_bytes;   /* header included */
+    int64_t header_bytes;
+    int32_t n_ref;
+    int32_t k_tags;
+    int32_t *ref, *pos, *end;
+    uint8_t* mapq;
+    uint16_t* flag;
+    int32_t *nref, *npos, *tlen, *l_seq;
+    uint16_t *clip_left, *clip_right;
+    uint8_t* tag_type;        /* k_tags * n_records each, tag-major, as cb_find_tags; NULL for k_tags = 0 */
+    int64_t* tag_voff;
+    int32_t* tag_vlen;
+    int64_t* tag_value;
+} cb_batch_file;
+
+/* Plan a batch of n_files BGZF-compressed BAM files, comp[i] (device) of comp_bytes[i] bytes, each a
+ * whole file; k <= 16 tags (2k characters in `tags`, host) are decoded with the columns.  Runs the
+ * first decode on `stream` to size every buffer (synchronises); the batch owns its device memory.
+ * Errors: the reference's status of the failing stage (truncated, corrupt block, inflate, CRC, no
+ * chain), CB_ERR_ARG for input that is not BAM. */
+int cb_batch_create(const uint8_t* const* comp, const int64_t* comp_bytes, int32_t n_files, const char* tags,
+                    int32_t k, int check_crc, void* stream, cb_batch** out);
+/* One decode of every file on `stream` (the captured graph when there is one); no synchronisation. */
+int cb_batch_run(cb_batch* b, void* stream);
+/* Record a run as a CUDA graph on `stream` (not the legacy default stream); later runs replay it. */
+int cb_batch_capture(cb_batch* b, void* stream);
+/* Synchronise `stream` and check the last run: every device status, and counts equal to the plan. */
+int cb_batch_check(cb_batch* b, void* stream);
+/* File i's results. */
+int cb_batch_file_info(const cb_batch* b, int32_t i, cb_batch_file* out);
+/* Inflate jobs of a run (all files), and the inflate form it uses. */
+int64_t cb_batch_total_jobs(const cb_batch* b);
+int cb_batch_form(const cb_batch* b);
+void cb_batch_destroy(cb_batch* b);
 
 #ifdef __cplusplus
 }

@@ -95,3 +95,45 @@ def test_batch_plan_forms_and_graph_replay(uneven):
         for a, b in zip(plan.results, ref):
             _same(a, b)
     assert plan.launches_per_run() > len(files)
+
+
+def test_native_batch_matches_decode_many(uneven):
+    """The batch planned and run by the library (cb_batch_*): results equal decode_many's, again after
+    eager runs and after graph replays that rewrite them in place."""
+    files = [(comp, hdr) for _, comp, hdr in uneven]
+    ref = batch.decode_many(files, tags=TAGS)
+    nb = batch.NativeBatch(files, tags=TAGS)
+    assert nb.form in (1, 2, 3)
+    for res, r in zip(nb.results, ref):
+        _same(res, r)
+        assert res.n_members == r.n_members and res.inflated_bytes == r.inflated_bytes
+    for res in nb.results:
+        res.columns["pos"].fill_(-7)
+        res.offset.fill_(-1)
+    nb.run()
+    nb.check()
+    for res, r in zip(nb.results, ref):
+        _same(res, r)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        nb.capture()
+        for res in nb.results:
+            res.columns["pos"].fill_(-7)
+            res.tags["CB"].offset.fill_(0)
+        for _ in range(2):
+            nb.run()
+        nb.check()
+    torch.cuda.synchronize()
+    for res, r in zip(nb.results, ref):
+        _same(res, r)
+    nb.close()
+
+
+def test_native_batch_errors(uneven):
+    _, comp, hdr = uneven[0]
+    with pytest.raises(ValueError, match="Truncated BGZF file"):
+        batch.NativeBatch([(comp[: comp.numel() - 100].clone(), hdr)], tags=TAGS)
+    bad = comp.clone()
+    bad[30:60] = 0  # inside the first member's DEFLATE data
+    with pytest.raises(ValueError, match="Corrupt BGZF block|No valid block"):
+        batch.NativeBatch([(bad, hdr)], tags=TAGS)

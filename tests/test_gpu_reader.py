@@ -170,7 +170,28 @@ def _payloads(seed: int):
     return out
 
 
-FORMS = [1, 2, 3]  # one member per warp, one member per lane, decode per lane + copy per warp
+# one member per warp, one member per lane, decode per lane + copy per warp (form 3 also with the copy
+# kernel's groups of 64 units, at 12 and 24 warps, and with the decoder's 8-bit root tables)
+FORMS = [1, 2, 3, "3/u2", "3/u2/w24", "3/r8"]
+_FORM_PARAMS = {"u": G._lib.PARAM_COPY_UNITS, "w": G._lib.PARAM_COPY_WARPS, "r": G._lib.PARAM_DECODE_ROOT}
+
+
+class _Form:
+    """An inflate form of FORMS with its launch parameters set, restored on exit."""
+
+    def __init__(self, spec):
+        parts = str(spec).split("/")
+        self.form = int(parts[0])
+        self.params = [(_FORM_PARAMS[x[0]], int(x[1:])) for x in parts[1:]]
+
+    def __enter__(self):
+        for key, v in self.params:
+            assert G._lib.lib.cb_set_param(key, v) == 0
+        return self.form
+
+    def __exit__(self, *exc):
+        for key, _ in self.params:
+            G._lib.lib.cb_set_param(key, -1)
 
 
 @pytest.mark.parametrize("form", FORMS)
@@ -203,8 +224,9 @@ def test_inflate_matches_zlib(tmp_path, level, strategy, form):
     assert s.status == 0 and s.n_members == len(payloads)
     assert s.total_out == sum(len(p) for p in payloads)
     out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
-    summ = G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form)
-    G.check_inflate(summ)
+    with _Form(form) as f:
+        summ = G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=f)
+        G.check_inflate(summ)
     assert _np(out).tobytes() == b"".join(payloads)
 
 
@@ -217,7 +239,8 @@ def test_inflate_output_alignment_and_offsets(form):
     for shift in range(18):
         jobs, s = G.scan_members(buf, True, out_base=shift)
         out = torch.zeros(shift + int(s.total_out), dtype=torch.uint8, device="cuda")
-        G.check_inflate(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form))
+        with _Form(form) as f:
+            G.check_inflate(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=f))
         assert _np(out[shift:]).tobytes() == b"".join(payloads)
         assert not bool(out[:shift].any())
 
@@ -237,8 +260,9 @@ def test_inflate_corrupt_members_are_errors(form):
         buf = torch.frombuffer(bytearray(bytes(m) + G.EOF_BLOCK), dtype=torch.uint8).cuda()
         jobs, s = G.scan_members(buf, True)
         out = torch.empty(int(s.total_out), dtype=torch.uint8, device="cuda")
-        st = int(G.read_struct(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=form),
-                               G._lib.InflateSummary).status)
+        with _Form(form) as f:
+            st = int(G.read_struct(G.inflate_jobs(jobs, int(s.n_jobs), out, True, form=f),
+                                   G._lib.InflateSummary).status)
         d = zlib.decompressobj(-15)
         try:
             z = d.decompress(bytes(m[18:-8]), len(data) + 1)
@@ -282,7 +306,8 @@ def test_inflate_many_members_all_forms_same_codes():
     for form in FORMS:
         out = torch.zeros(int(s.total_out), dtype=torch.uint8, device="cuda")
         codes = torch.full((n,), 99, dtype=torch.int32, device="cuda")
-        summ = G.read_struct(G.inflate_jobs(jobs, n, out, True, form=form, job_status=codes), G._lib.InflateSummary)
+        with _Form(form) as f:
+            summ = G.read_struct(G.inflate_jobs(jobs, n, out, True, form=f, job_status=codes), G._lib.InflateSummary)
         codes = codes.cpu().numpy()
         assert (codes != 99).all()
         assert int(summ.n_bad) == int((codes != 0).sum())
