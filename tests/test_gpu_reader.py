@@ -354,3 +354,25 @@ def test_fused_record_pass_equals_the_separate_decoders(name, chunk):
         idx = torch.arange(0, len(b), 3, device="cuda")
         t = f.take(idx)
         assert torch.equal(t.aligned_length(), b.take(idx).aligned_length())
+
+
+def test_too_many_member_candidates():
+    """More than n/28 + 1024 member header matches in a chunk: the reference's "Too many candidates"
+    error (src/cubam/bgzf.py:554, src/cubam/_kernels.py:671), as the oracle gives it, through the scan
+    and through read_bam."""
+    import tempfile
+
+    from test_oracle import _fake_headers
+
+    raw = _fake_headers(8000)
+    with pytest.raises(ValueError, match="Too many candidates: the data is corrupt"):
+        O.scan_members(raw, True)
+    _, s = G.scan_members(torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda(), True)
+    assert s.status == G._lib.TOO_MANY
+    with pytest.raises(ValueError, match="Too many candidates: the data is corrupt"):
+        G.raise_status(s.status, "scan")
+    with tempfile.NamedTemporaryFile(suffix=".bam") as f:
+        f.write(raw)
+        f.flush()
+        with pytest.raises(ValueError, match="Too many candidates: the data is corrupt"):
+            list(cubam_b200.inflate_chunks(f.name))

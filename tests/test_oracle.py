@@ -127,3 +127,22 @@ def test_truncated_bam_raises():
     cut = member(data[:-10])
     with pytest.raises(ValueError, match="truncated BAM file"):
         list(O.read_bam(cut, 1 << 20))
+
+
+def _fake_headers(count: int) -> bytes:
+    """A chunk of BGZF member headers every 18 bytes, each claiming a 26-byte member: far more header
+    matches than a real chunk holds (at least 28 bytes per member)."""
+    import struct
+
+    return (bytes.fromhex("1f8b08040000000000ff060042430200") + struct.pack("<H", 25)) * count
+
+
+def test_too_many_member_candidates():
+    """The reference raises "Too many candidates" when a chunk holds more than n/28 + 1024 member
+    header matches (src/cubam/bgzf.py:554, src/cubam/_kernels.py:671); the oracle does the same."""
+    with pytest.raises(ValueError, match="Too many candidates: the data is corrupt"):
+        O.scan_members(_fake_headers(8000), True)
+    few = _fake_headers(1000)  # 18,000 bytes: 1,000 matches, under 18,000 / 28 + 1024
+    with pytest.raises(ValueError) as e:
+        O.scan_members(few, True)
+    assert "Too many" not in str(e.value)
