@@ -37,7 +37,7 @@ constexpr Param kParams[] = {
     {CB_PARAM_DECODE_STEPS, 1, 64, 16},
     {CB_PARAM_DECODE_PREFETCH, 0, 16, 4},
     {CB_PARAM_SPLIT_MIN_JOBS, 0, 1LL << 40, 30000},
-    {CB_PARAM_COPY_UNITS, 1, 2, 1},
+    {CB_PARAM_COPY_UNITS, 1, 4, 2},
 };
 constexpr int kNParams = sizeof(kParams) / sizeof(kParams[0]);
 std::atomic<int64_t> g_param[kNParams] = {};
@@ -69,6 +69,8 @@ extern "C" int cb_set_param(int key, int64_t value) {
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
     if (key == CB_PARAM_CHAIN_TILE && value && (value < 2048 || (value & (value - 1))))
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two from 2048 to 32768");
+    if (key == CB_PARAM_COPY_UNITS && value == 3)
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy units per lane are 1, 2 or 4");
     if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6 && value != 12 && value != 24)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy warps per CTA are 2, 3, 6, 12 or 24");
     g_param[i].store(value, std::memory_order_relaxed);

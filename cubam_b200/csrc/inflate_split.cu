@@ -1049,7 +1049,7 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
             rc = launch_decode<split::DecCfg<6, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
         if (rc != CB_OK) return rc;
         const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
-        const bool two = cb_param(CB_PARAM_COPY_UNITS) == 2;
+        const int units = (int)cb_param(CB_PARAM_COPY_UNITS);
 #define CB_COPY(W, R, UPL) \
     launch_copy<split::CopyCfg<W, R, UPL>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s)
         if (cw == 2)
@@ -1057,11 +1057,11 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
         else if (cw == 3)
             rc = CB_COPY(3, 16384, 1);
         else if (cw == 12)
-            rc = two ? CB_COPY(12, 8192, 2) : CB_COPY(12, 8192, 1);
+            rc = units == 4 ? CB_COPY(12, 8192, 4) : units == 2 ? CB_COPY(12, 8192, 2) : CB_COPY(12, 8192, 1);
         else if (cw == 24)
-            rc = two ? CB_COPY(24, 4096, 2) : CB_COPY(24, 4096, 1);
+            rc = units >= 2 ? CB_COPY(24, 4096, 2) : CB_COPY(24, 4096, 1);
         else
-            rc = two ? CB_COPY(6, 16384, 2) : CB_COPY(6, 16384, 1);
+            rc = units == 4 ? CB_COPY(6, 16384, 4) : units == 2 ? CB_COPY(6, 16384, 2) : CB_COPY(6, 16384, 1);
 #undef CB_COPY
         if (rc != CB_OK) return rc;
     }

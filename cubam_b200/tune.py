@@ -33,7 +33,7 @@ CANDIDATES = {
     "inflate_form": (_lib.PARAM_INFLATE_FORM, (1, 2, 3)),
     "decode_root": (_lib.PARAM_DECODE_ROOT, (6, 7, 8)),
     "copy_warps": (_lib.PARAM_COPY_WARPS, (6, 12, 24)),
-    "copy_units": (_lib.PARAM_COPY_UNITS, (1, 2)),
+    "copy_units": (_lib.PARAM_COPY_UNITS, (1, 2, 4)),
     "decode_steps": (_lib.PARAM_DECODE_STEPS, (8, 16, 32)),
     "decode_prefetch": (_lib.PARAM_DECODE_PREFETCH, (0, 4, 8)),
     "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 4096, 16384)),

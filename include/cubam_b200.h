@@ -103,7 +103,8 @@ int cb_device_sm_count(void);
  *                          (form 3 decodes one member per lane, so it needs many members to fill the GPU):
  *                          0 or more (30000)
  *   CB_PARAM_COPY_UNITS    DEFLATE units each lane of form 3's copy kernel takes per group: 1 (groups of
- *                          32 units) or 2 (groups of 64, with 6, 12 or 24 copy warps) (1)
+ *                          32 units), 2 (64; with 6, 12 or 24 copy warps) or 4 (128; with 6 or 12 copy
+ *                          warps, else 2) (2)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {

@@ -58,6 +58,7 @@ def test_launch_parameters_are_checked_and_restored():
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 3000) == _lib.ARG  # not a power of two
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 1 << 16) == _lib.ARG  # above 32 KiB
     assert L.cb_set_param(_lib.PARAM_COPY_WARPS, 4) == _lib.ARG
+    assert L.cb_set_param(_lib.PARAM_COPY_UNITS, 3) == _lib.ARG
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 8192) == _lib.OK
     assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 8192
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 1024) == _lib.ARG
@@ -65,5 +66,5 @@ def test_launch_parameters_are_checked_and_restored():
     assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 0
     for key, default in ((_lib.PARAM_INFLATE_FORM, 3), (_lib.PARAM_DECODE_ROOT, 7), (_lib.PARAM_COPY_WARPS, 12),
                          (_lib.PARAM_DECODE_STEPS, 16), (_lib.PARAM_DECODE_PREFETCH, 4),
-                         (_lib.PARAM_SPLIT_MIN_JOBS, 30000), (_lib.PARAM_COPY_UNITS, 1)):
+                         (_lib.PARAM_SPLIT_MIN_JOBS, 30000), (_lib.PARAM_COPY_UNITS, 2)):
         assert L.cb_get_param(key) == default
