@@ -30,7 +30,7 @@ struct Param {
     int64_t lo, hi, def;
 };
 constexpr Param kParams[] = {
-    {CB_PARAM_CHAIN_TILE, 0, 32768, 0},
+    {CB_PARAM_CHAIN_TILE, 0, 65536, 0},
     {CB_PARAM_INFLATE_FORM, 1, 3, 3},
     {CB_PARAM_DECODE_ROOT, 6, 8, 7},
     {CB_PARAM_COPY_WARPS, 2, 24, 12},
@@ -68,7 +68,7 @@ extern "C" int cb_set_param(int key, int64_t value) {
     if (value < kParams[i].lo || value > kParams[i].hi)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: value out of range");
     if (key == CB_PARAM_CHAIN_TILE && value && (value < 2048 || (value & (value - 1))))
-        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two from 2048 to 32768");
+        return cb_set_error_text(CB_ERR_ARG, "cb_set_param: the chain tile is 0 (by size) or a power of two from 2048 to 65536");
     if (key == CB_PARAM_COPY_UNITS && value == 3)
         return cb_set_error_text(CB_ERR_ARG, "cb_set_param: copy units per lane are 1, 2 or 4");
     if (key == CB_PARAM_COPY_WARPS && value != 2 && value != 3 && value != 6 && value != 12 && value != 24)

@@ -4,14 +4,16 @@
 // cubam tests the record predicate (is_record, src/cubam/_kernels.py:250-278) at every byte offset and
 // keeps the chain from offset 0.  Only offsets on that chain matter: the result is the walk from 0 that
 // follows block_size while the predicate holds, which is O(records), not O(bytes).  It is walked in
-// parallel by tiles of CB_PARAM_CHAIN_TILE bytes (by default 8 KB, less for small chunks):
+// parallel by tiles of CB_PARAM_CHAIN_TILE bytes (by default 64 KB, less for small chunks):
 //
-//  1. k_walk: one warp per tile.  The tile's bytes (and a little after it) are copied to shared
-//     memory with coalesced 16-byte loads; the lanes test 32 offsets at a time for the tile's first
-//     offset that passes the predicate; one lane follows the block_size links from it in shared
-//     memory up to the first offset past the tile; then the lanes test the predicate on those records
-//     in parallel.  Out: first[t], count[t] (up to the first record that fails), exit[t], whether the
-//     walk broke inside the tile, and the records' offsets in the tile (16-bit, relative to it).
+//  1. k_walk: one warp per tile, the tile staged in shared memory 8 KB at a time (coalesced
+//     asynchronous 16-byte copies; the window slides on as the walk passes it).  The lanes test 32
+//     offsets at a time for the tile's first offset that passes the predicate; one lane follows the
+//     block_size links from it through the window up to the first offset past the tile; the lanes
+//     test the predicate on each window's records in parallel.  Out: first[t], count[t] (up to the
+//     first record that fails), exit[t], whether the walk broke inside the tile, and the records'
+//     offsets in the tile (16-bit, relative to it).  Tiles of 64 KB hold about 256 records, so one
+//     first-record search serves many links.
 //  2. k_check: tile t's walk is the true chain when its first offset is where the previous non-empty
 //     tile's walk left (exit); a tile whose candidate is not on the chain (a spurious match of the
 //     predicate) makes the chunk take the serial path.  With none (the usual case, none were seen in
@@ -29,18 +31,22 @@ namespace cb {
 namespace chain {
 
 constexpr long long T_MIN = 2048;   // smallest tile
-constexpr long long T_MAX = 32768;  // largest tile (shared memory per warp)
+constexpr long long T_MAX = 65536;  // largest tile (record offsets are kept as 16 bits from the tile start)
 constexpr int NT = 256;
 constexpr int WW = 4;               // warps per block of k_walk
-constexpr int HALO = 512;           // bytes staged after the tile (headers of records that cross its end)
+constexpr int WIN = 8192;           // bytes of a tile staged at a time (the walk slides the window)
+constexpr int HALO = 512;           // bytes staged after the window (headers of records that cross its end)
+constexpr int HEAD = 40;            // bytes of a record header the hop loop wants inside the window
 constexpr int SCAN = 1024;          // tiles per block of the count scan
 constexpr int MIN_RECORD = 37;      // bytes of the shortest record the predicate accepts (block_size >= 33)
 
 // Record offsets one tile can hold (records are at least MIN_RECORD bytes apart).
 __host__ __device__ inline long long rel_cap(long long T) { return T / MIN_RECORD + 2; }
-// Shared memory of one k_walk warp: the staged bytes (plus slack for word reads), the relative offsets.
-__host__ __device__ inline long long stage_bytes_for(long long T) { return ((T + HALO + 32 + 15) / 16) * 16; }
-__host__ __device__ inline long long warp_smem(long long T) { return stage_bytes_for(T) + ((rel_cap(T) * 2 + 15) / 16) * 16; }
+// Shared memory of one k_walk warp: the staged window (plus slack for word reads) and the offsets of
+// the records that start in it.
+constexpr int STAGE_BYTES = ((WIN + HALO + 32 + 15) / 16) * 16;
+constexpr int LIST = (WIN + HALO) / MIN_RECORD + 2;
+constexpr int WARP_SMEM = STAGE_BYTES + ((LIST * 2 + 15) / 16) * 16;
 
 struct Ws {
     int64_t* first;    // per tile
@@ -153,20 +159,27 @@ __global__ void k_init(Ws w) {
     w.meta[3] = 0;
 }
 
+// A warp per tile, the tile's bytes staged a window at a time.
 __global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b, long long n, int n_ref, Ws w) {
     extern __shared__ uint4 walk_mem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long T = w.T, sb = stage_bytes_for(T);
-    uint4* st = walk_mem + (size_t)warp * (warp_smem(T) / 16);
-    uint16_t* rel = reinterpret_cast<uint16_t*>(reinterpret_cast<uint8_t*>(st) + sb);
+    uint4* st = walk_mem + (size_t)warp * (WARP_SMEM / 16);
+    uint16_t* list = reinterpret_cast<uint16_t*>(reinterpret_cast<uint8_t*>(st) + STAGE_BYTES);
+    const uint8_t* sb = reinterpret_cast<const uint8_t*>(st);
     for (long long t = (long long)blockIdx.x * WW + warp; t < w.ntiles; t += (long long)gridDim.x * WW) {
-        const long long ts = t * T, te = min(ts + T, n);
-        const long long hi = min(te + HALO, n);
-        const long long r0 = stage_bytes(b, ts, hi, st);
-        const StagedBytes d{b, reinterpret_cast<const uint8_t*>(st), r0, hi};
-        // the tile's first offset that passes the predicate, 32 offsets at a time
+        const long long T = w.T, ts = t * T, te = min(ts + T, n);
+        long long hi = min(ts + WIN + HALO, n);
+        long long r0 = stage_bytes(b, ts, hi, st);
+        // the tile's first offset that passes the predicate, 32 offsets at a time (the window slides
+        // on when the search passes it)
         long long c = -1;
         for (long long base = ts; base < te; base += 32) {
+            if (base + 32 + HEAD > hi && hi < n) {
+                __syncwarp();
+                hi = min(base + WIN + HALO, n);
+                r0 = stage_bytes(b, base, hi, st);
+            }
+            const StagedBytes d{b, sb, r0, hi};
             const long long o = base + lane;
             bool ok = false;
             if (o < te && o + 4 <= n) {
@@ -183,39 +196,69 @@ __global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b,
         bool broken = false;
         long long exit = -1;
         if (c >= 0) {
-            // one lane follows the links; a link that cannot be a record ends the list (the predicate
-            // fails there below)
-            int m = 0;
             long long o = c;
-            if (lane == 0) {
-                while (o < te) {
-                    rel[m++] = (uint16_t)(o - ts);
-                    const uint32_t bs = o + 4 <= n ? d.u32(o) : 0u;
-                    if (o + 36 > n || bs < 33 || bs > (1u << 22) || o + 4 + (long long)bs > n) break;
-                    o += 4 + (long long)bs;
+            for (;;) {
+                if (o + HEAD > hi && hi < n) {  // the next header is past the window: slide it on
+                    __syncwarp();
+                    hi = min(o + WIN + HALO, n);
+                    r0 = stage_bytes(b, o, hi, st);
                 }
-            }
-            m = __shfl_sync(FULL, m, 0);
-            o = __shfl_sync(FULL, o, 0);
-            __syncwarp();
-            // the predicate on the listed records, in parallel: the count ends at the first failure
-            int f = m;
-            for (int j0 = 0; j0 < m; j0 += 32) {
-                const int j = j0 + lane;
-                const bool ok = j >= m || is_record_at(d, n, ts + rel[j], n_ref);
-                const unsigned bad = __ballot_sync(FULL, !ok);
-                if (bad) {
-                    f = j0 + __ffs(bad) - 1;
+                // one lane follows the links while their headers are in the window; a link that cannot
+                // be a record ends the list (the predicate fails there below)
+                int m = 0;
+                bool stop = false;
+                if (lane == 0) {
+                    while (o < te && (o + HEAD <= hi || hi >= n)) {
+                        list[m++] = (uint16_t)(o - ts);
+                        uint32_t bs = 0;
+                        if (o + 4 <= hi) {  // block_size from the window: byte x of the data is sb[x - r0]
+                            const long long q = o - r0;
+                            const uint32_t* wd = reinterpret_cast<const uint32_t*>(sb + (q & ~3LL));
+                            bs = __funnelshift_r(wd[0], wd[1], (unsigned)(q & 3) * 8);
+                        }
+                        if (o + 36 > n || bs < 33 || bs > (1u << 22) || o + 4 + (long long)bs > n) {
+                            stop = true;
+                            break;
+                        }
+                        o += 4 + (long long)bs;
+                    }
+                }
+                m = __shfl_sync(FULL, m, 0);
+                o = __shfl_sync(FULL, o, 0);
+                stop = __shfl_sync(FULL, (int)stop, 0) != 0;
+                __syncwarp();
+                // the predicate on the listed records, in parallel: the count ends at the first failure
+                const StagedBytes d{b, sb, r0, hi};
+                int f = m;
+                for (int j0 = 0; j0 < m; j0 += 32) {
+                    const int j = j0 + lane;
+                    const bool ok = j >= m || is_record_at(d, n, ts + list[j], n_ref);
+                    const unsigned bad = __ballot_sync(FULL, !ok);
+                    if (bad) {
+                        f = j0 + __ffs(bad) - 1;
+                        break;
+                    }
+                }
+                if (stop && f == m) f = m - 1;  // a link that fails its checks fails the predicate too
+                for (int j = lane; j < f; j += 32) w.rel[t * w.rcap + cnt + j] = list[j];
+                cnt += f;
+                __syncwarp();
+                if (f < m) {
+                    broken = true;
+                    exit = ts + list[f];
+                    break;
+                }
+                if (o >= te) {
+                    exit = o;
                     break;
                 }
             }
-            cnt = f;
-            broken = f < m;
-            exit = broken ? ts + rel[f] : o;
-            for (int j = lane; j < cnt; j += 32) w.rel[t * w.rcap + j] = rel[j];
         }
         if (lane == 0) {
-            if (c >= 0) atomicOr(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
+            // one flag for the whole chunk: read it first, so that the tiles do not all queue on one
+            // address
+            if (c >= 0 && *reinterpret_cast<volatile int64_t*>(&w.meta[2]) == 0)
+                atomicOr(reinterpret_cast<unsigned long long*>(&w.meta[2]), 1ull);
             if (broken) atomicMin(reinterpret_cast<long long*>(&w.meta[1]), t);
             w.first[t] = c;
             w.exit[t] = exit;
@@ -387,21 +430,21 @@ extern "C" int cb_record_chain(const uint8_t* data, int64_t n, int32_t n_ref, in
     long long tile = cb_param(CB_PARAM_CHAIN_TILE);
     const long long sms = cb_device_sm_count();
     if (tile == 0) {
-        // 8 KB tiles (a warp stages one, about 32 records), smaller ones for chunks too small to give
-        // 32 tiles per SM
-        tile = 8192;
-        while (tile > chain::T_MIN && n / tile < sms * 32) tile /= 2;
+        // 64 KB tiles (about 256 records: one first-record search per tile), smaller ones for chunks
+        // too small to give 16 tiles per SM
+        tile = chain::T_MAX;
+        while (tile > chain::T_MIN && n / tile < sms * 16) tile /= 2;
     }
     if (tile < chain::T_MIN || tile > chain::T_MAX || (tile & (tile - 1))) return CB_ERR_ARG;
     chain::Ws w = chain::carve(workspace, n, tile);
-    const size_t smem = (size_t)chain::WW * chain::warp_smem(tile);
+    const size_t smem = (size_t)chain::WW * chain::WARP_SMEM;
     {
         static std::atomic<bool> attr_set[64];
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64 || !attr_set[dev].load(std::memory_order_acquire)) {
             const cudaError_t e = cudaFuncSetAttribute(chain::k_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)(chain::WW * chain::warp_smem(chain::T_MAX)));
+                                                       (int)smem);
             if (e != cudaSuccess) return cb_set_error(e);
             if (dev >= 0 && dev < 64) attr_set[dev].store(true, std::memory_order_release);
         }

@@ -5,13 +5,14 @@
 //  1. k_scan_count: a warp per 4 KB tile; each lane loads its eight 16-byte chunks with 128-bit
 //     loads, then __vcmpeq4 finds 0x1f bytes (about 1 in 256 in compressed data) and only those
 //     offsets get the full header test.  The count of every tile goes to the workspace.
-//  2. k_scan_tiles: one block turns the tile counts into tile offsets (prefix sum; each thread
-//     sums a contiguous run of tiles).
+//  2. k_scan_tiles: one block turns the tile counts into tile offsets (prefix sum; each warp
+//     takes a contiguous segment, read coalesced with eight loads per lane in flight).
 //  3. k_scan_write: tiles with candidates are tested again and their offsets written in order
 //     (block prefix sum of the per-thread counts); no sort is needed.
-//  4. k_scan_finish: one block keeps the chain from offset 0 (all candidates in the usual case,
-//     otherwise a walk), applies the reference's checks in the reference's order and writes the
-//     inflate jobs of the non-empty members with their output offsets (prefix sum of ISIZE).
+//  4. k_fin_sums, k_scan_finish, k_fin_jobs: the chain from offset 0 (all candidates in the usual
+//     case, checked and summed per block of candidates by a grid; otherwise a walk in one block),
+//     the reference's checks in the reference's order, and the inflate jobs of the non-empty members
+//     with their output offsets (prefix sum of ISIZE), written by a grid.
 
 #include <atomic>
 
@@ -139,21 +140,58 @@ __global__ void __launch_bounds__(NT) k_scan_count(const uint8_t* buf, long long
     }
 }
 
-// Exclusive prefix sum of the tile counts (one block, each thread a contiguous run of tiles);
-// meta[0] = total, meta[1] = status.
+// Exclusive prefix sum of the tile counts (one block); meta[0] = total, meta[1] = status.  Each warp
+// takes a contiguous segment of tiles, read coalesced with eight loads per lane in flight: a first
+// pass sums the segment, the warps' sums are scanned, and a second pass writes the offsets.
 __global__ void __launch_bounds__(FIN_NT) k_scan_tiles(Ws w, long long too_many) {
-    __shared__ int64_t sm[33];
-    const long long per = (w.ntiles + FIN_NT - 1) / FIN_NT;
-    const long long a = min((long long)threadIdx.x * per, w.ntiles), b = min(a + per, w.ntiles);
+    constexpr int NW = FIN_NT / 32, U = 8;
+    __shared__ int64_t wbase[NW + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long seg = ((w.ntiles + NW - 1) / NW + 32 * U - 1) / (32 * U) * (32 * U);
+    const long long a = min((long long)warp * seg, w.ntiles), b = min(a + seg, w.ntiles);
     int64_t sum = 0;
-    for (long long i = a; i < b; i++) sum += w.tile_count[i];
-    int64_t tot;
-    int64_t x = block_exclusive_scan<FIN_NT>(sum, tot, sm);
-    for (long long i = a; i < b; i++) {
-        w.tile_off[i] = x;
-        x += w.tile_count[i];
+    for (long long i0 = a; i0 < b; i0 += 32 * U) {
+        uint32_t v[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long i = i0 + k * 32 + lane;
+            v[k] = i < b ? w.tile_count[i] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) sum += v[k];
+    }
+    for (int d = 16; d; d >>= 1) sum += __shfl_xor_sync(FULL, sum, d);
+    if (lane == 0) wbase[warp] = sum;
+    __syncthreads();
+    if (warp == 0) {
+        const int64_t x = lane < NW ? wbase[lane] : 0;
+        int64_t tot;
+        const int64_t e = warp_exclusive_scan(x, tot);
+        __syncwarp();
+        if (lane < NW) wbase[lane] = e;
+        if (lane == 0) wbase[NW] = tot;
+    }
+    __syncthreads();
+    int64_t carry = wbase[warp];
+    for (long long i0 = a; i0 < b; i0 += 32 * U) {
+        uint32_t v[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long i = i0 + k * 32 + lane;
+            v[k] = i < b ? w.tile_count[i] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long i = i0 + k * 32 + lane;
+            int64_t t;
+            const int64_t x = warp_exclusive_scan((int64_t)v[k], t);
+            if (i < b) w.tile_off[i] = carry + x;
+            carry += t;
+        }
     }
     if (threadIdx.x == 0) {
+        const int64_t tot = wbase[NW];
+        w.meta[2] = 0;  // set by the finish when k_fin_jobs is to write the jobs
         w.meta[0] = tot;
         w.meta[1] = tot > too_many ? CB_ERR_TOO_MANY : (tot > w.cap ? CB_ERR_CAPACITY : CB_OK);
     }
@@ -187,6 +225,103 @@ __device__ __forceinline__ long long lower_bound(const int64_t* a, long long m, 
     return lo;
 }
 
+// ---- the finish: chain check, the reference's checks, the job table
+//
+// The usual case is that every candidate ends where the next one starts.  k_fin_sums (a grid) checks
+// that for blocks of FIN_NT candidates and sums each block's jobs and output bytes into the tile
+// arrays (free once the candidates are written); k_scan_finish (one block) scans those sums and
+// applies the checks, or, when a link breaks, keeps the chain from offset 0 by a walk and writes the
+// jobs itself; k_fin_jobs (a grid) writes the jobs of the all-chained case.
+
+// Candidates' block b: sums at tile_off[2b] (jobs) and tile_off[2b + 1] (output bytes); flags at
+// tile_count[b]: bit 0 a broken link, bit 1 a bad member (ISIZE too large, or an empty member that is
+// not the EOF block's form).
+__device__ __forceinline__ void member_fields(const uint8_t* buf, const Ws& w, long long i, long long& c,
+                                              long long& bs, int64_t& isz, bool& bad) {
+    c = w.cand[i];
+    bs = (long long)ld_u16(buf, c + 16) + 1;
+    isz = (int64_t)ld_u32(buf, c + bs - 4);
+    bad = isz > MAX_ISIZE || (isz == 0 && (bs != 28 || buf[c + 18] != 3 || buf[c + 19] != 0));
+}
+
+// Whether the block sums of m candidates fit the tile arrays (2 per block in tile_off); below about
+// 17 KB of input they may not, and the finish takes the single-block path.
+__device__ __forceinline__ bool fin_sums_fit(const Ws& w, long long m) {
+    return 2 * ((m + FIN_NT - 1) / FIN_NT) <= w.ntiles;
+}
+
+__global__ void __launch_bounds__(FIN_NT) k_fin_sums(const uint8_t* buf, Ws w) {
+    __shared__ int64_t sm[33];
+    __shared__ uint32_t s_flags;
+    if (w.meta[1] != CB_OK) return;
+    const long long m = w.meta[0];
+    if (!fin_sums_fit(w, m)) return;
+    const long long nb = (m + FIN_NT - 1) / FIN_NT;
+    for (long long b = blockIdx.x; b < nb; b += gridDim.x) {
+        if (threadIdx.x == 0) s_flags = 0;
+        __syncthreads();
+        const long long i = b * FIN_NT + threadIdx.x;
+        int64_t is_job = 0, out = 0;
+        uint32_t flags = 0;
+        if (i < m) {
+            long long c, bs;
+            int64_t isz;
+            bool bad;
+            member_fields(buf, w, i, c, bs, isz, bad);
+            if (i + 1 < m && c + bs != w.cand[i + 1]) flags |= 1;
+            if (bad) flags |= 2;
+            is_job = isz > 0 && isz <= MAX_ISIZE;
+            out = is_job ? isz : 0;
+        }
+        if (flags) atomicOr(&s_flags, flags);
+        int64_t tj, to;
+        block_exclusive_scan<FIN_NT>(is_job, tj, sm);
+        block_exclusive_scan<FIN_NT>(out, to, sm);
+        if (threadIdx.x == 0) {
+            w.tile_off[2 * b] = tj;
+            w.tile_off[2 * b + 1] = to;
+            w.tile_count[b] = s_flags;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(FIN_NT) k_fin_jobs(const uint8_t* buf, long long out_base, cb_member_job* jobs,
+                                                    long long jobs_cap, Ws w) {
+    __shared__ int64_t sm[33];
+    if (w.meta[1] != CB_OK || w.meta[2] != 1) return;  // not the all-chained case, or already failed
+    const long long m = w.meta[0];
+    const long long nb = (m + FIN_NT - 1) / FIN_NT;
+    for (long long b = blockIdx.x; b < nb; b += gridDim.x) {
+        const long long i = b * FIN_NT + threadIdx.x;
+        int64_t is_job = 0, out = 0;
+        long long c = 0, bs = 0;
+        int64_t isz = 0;
+        if (i < m) {
+            bool bad;
+            member_fields(buf, w, i, c, bs, isz, bad);
+            is_job = isz > 0 && isz <= MAX_ISIZE;
+            out = is_job ? isz : 0;
+        }
+        int64_t tj, to;
+        const int64_t xj = block_exclusive_scan<FIN_NT>(is_job, tj, sm);
+        const int64_t xo = block_exclusive_scan<FIN_NT>(out, to, sm);
+        if (is_job) {
+            const long long k = w.tile_off[2 * b] + xj;
+            if (k < jobs_cap) {
+                cb_member_job j;
+                j.in = buf + c + 18;
+                j.out_off = out_base + w.tile_off[2 * b + 1] + xo;
+                j.in_len = (uint32_t)(bs - 26);
+                j.isize = (uint32_t)isz;
+                j.crc = ld_u32(buf, c + bs - 8);
+                j.reserved = 0;
+                jobs[k] = j;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(FIN_NT) k_scan_finish(const uint8_t* buf, long long n, int eof, long long out_base,
                                                        cb_member_job* jobs, long long jobs_cap,
                                                        cb_scan_summary* summary, Ws w) {
@@ -213,15 +348,55 @@ __global__ void __launch_bounds__(FIN_NT) k_scan_finish(const uint8_t* buf, long
         if (tid == 0) summary->status = status;
         return;
     }
-    // fast path: every candidate ends where the next starts
-    int local = 0;
-    for (long long i = tid; i + 1 < m; i += FIN_NT) {
-        long long c = w.cand[i];
-        long long bs = (long long)ld_u16(buf, c + 16) + 1;
-        if (c + bs != w.cand[i + 1]) local = 1;
+    // does every candidate end where the next starts?  From the block flags of k_fin_sums, or (chunks
+    // too small for its sums to fit the tile arrays) by this block
+    const long long nb = (m + FIN_NT - 1) / FIN_NT;
+    const bool sums = fin_sums_fit(w, m);
+    uint32_t local = 0;
+    if (sums) {
+        for (long long b = tid; b < nb; b += FIN_NT) local |= w.tile_count[b];
+    } else {
+        for (long long i = tid; i + 1 < m; i += FIN_NT) {
+            const long long c = w.cand[i];
+            if (c + (long long)ld_u16(buf, c + 16) + 1 != w.cand[i + 1]) local |= 1;
+        }
     }
-    if (local) atomicOr(&s_breaks, 1);
+    if (local & 1) atomicOr(&s_breaks, 1);
     __syncthreads();
+    if (sums && s_breaks == 0) {
+        // all chained: scan the block sums into block bases (k_fin_jobs writes the jobs)
+        int64_t cj = 0, co = 0;
+        for (long long b0 = 0; b0 < nb; b0 += FIN_NT) {
+            const long long b = b0 + tid;
+            const int64_t vj = b < nb ? w.tile_off[2 * b] : 0, vo = b < nb ? w.tile_off[2 * b + 1] : 0;
+            int64_t tj, to;
+            const int64_t xj = block_exclusive_scan<FIN_NT>(vj, tj, sm);
+            const int64_t xo = block_exclusive_scan<FIN_NT>(vo, to, sm);
+            if (b < nb) {
+                w.tile_off[2 * b] = cj + xj;
+                w.tile_off[2 * b + 1] = co + xo;
+            }
+            cj += tj;
+            co += to;
+        }
+        if (tid == 0) {
+            const long long c = w.cand[m - 1];
+            const long long used = c + (long long)ld_u16(buf, c + 16) + 1;
+            int st = CB_OK;
+            if (eof && used != n) st = CB_ERR_TRUNCATED;
+            else if (local & 2) st = CB_ERR_CORRUPT_BLOCK;
+            else if (cj > jobs_cap) st = CB_ERR_CAPACITY;
+            summary->status = st;
+            if (st != CB_ERR_TRUNCATED) {
+                summary->n_members = m;
+                summary->n_jobs = cj;
+                summary->used = used;
+                summary->total_out = co;
+                w.meta[2] = 1;  // k_fin_jobs writes the jobs (those below jobs_cap)
+            }
+        }
+        return;
+    }
     if (s_breaks) {
         for (long long i = tid; i < m; i += FIN_NT) w.keep[i] = 0;
         __syncthreads();
@@ -332,7 +507,10 @@ extern "C" int cb_scan_members(const uint8_t* buf, int64_t n, int eof, int64_t o
     scan::k_scan_count<<<(unsigned)cgrid, scan::NT, 0, s>>>(buf, n, w);
     scan::k_scan_tiles<<<1, scan::FIN_NT, 0, s>>>(w, scan::cand_cap(n));
     scan::k_scan_write<<<(unsigned)grid, scan::NT, 0, s>>>(buf, n, w);
+    long long fgrid = (long long)sms * 2;
+    scan::k_fin_sums<<<(unsigned)fgrid, scan::FIN_NT, 0, s>>>(buf, w);
     scan::k_scan_finish<<<1, scan::FIN_NT, 0, s>>>(buf, n, eof, out_base_off, jobs, cap, summary, w);
+    scan::k_fin_jobs<<<(unsigned)fgrid, scan::FIN_NT, 0, s>>>(buf, out_base_off, jobs, cap, w);
     return cb_set_error(cudaGetLastError());
 }
 

@@ -36,7 +36,7 @@ CANDIDATES = {
     "copy_units": (_lib.PARAM_COPY_UNITS, (1, 2, 4)),
     "decode_steps": (_lib.PARAM_DECODE_STEPS, (8, 16, 32)),
     "decode_prefetch": (_lib.PARAM_DECODE_PREFETCH, (0, 4, 8)),
-    "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 4096, 16384)),
+    "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 16384, 32768)),
 }
 #: the stage each parameter is timed on (StageEvents names)
 STAGE = {"chain_tile": "chained"}

@@ -89,9 +89,9 @@ int cb_device_sm_count(void);
  *      src/cubam/_memory.py:11-23) ---------------------------------------------------------------
  * One value per key for the whole process, read by every later launch; the package's autotuner
  * times candidates on a workload and sets the fastest.  Workspace sizes never depend on them.
- *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk (a warp stages one in shared
- *                          memory): a power of two, 2-32 KiB, or 0: 8 KiB, less for chunks too small
- *                          to give 32 tiles per SM (0)
+ *   CB_PARAM_CHAIN_TILE    bytes per tile of the record chain's walk (a warp walks one, staging it in
+ *                          shared memory 8 KiB at a time): a power of two, 2-64 KiB, or 0: 64 KiB,
+ *                          less for chunks too small to give 16 tiles per SM (0)
  *   CB_PARAM_INFLATE_FORM  the form cb_inflate runs: 1 member per warp, 2 per lane, 3 split (3)
  *   CB_PARAM_DECODE_ROOT   literal/length root bits of form 3's lane decoder: 6, 7 or 8 (7)
  *   CB_PARAM_COPY_WARPS    warps per CTA of form 3's copy kernel: 2, 3 or 6 with a 16 KiB window per
@@ -200,7 +200,7 @@ int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d
 size_t cb_record_chain_workspace_bytes(int64_t n);
 
 /* Offsets of the complete records of data[0:n) on the chain from offset 0, under the reference's
- * record predicate (is_record, src/cubam/_kernels.py:250-278): walked by 2 KB tiles in parallel and
+ * record predicate (is_record, src/cubam/_kernels.py:250-278): walked by tiles in parallel and
  * stitched, O(records).  Writes offsets[0:cap) (cap >= n / 37 + 1 always suffices) and *summary.
  * cubam's "Too many candidates" error (more than n/32 + 1024 offsets passing the predicate) is not
  * raised: the walk never tests every offset. */

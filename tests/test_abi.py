@@ -56,7 +56,7 @@ def test_launch_parameters_are_checked_and_restored():
     assert L.cb_get_param(99) == -1
     assert L.cb_set_param(99, 1) == _lib.ARG
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 3000) == _lib.ARG  # not a power of two
-    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 1 << 16) == _lib.ARG  # above 32 KiB
+    assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 1 << 17) == _lib.ARG  # above 64 KiB
     assert L.cb_set_param(_lib.PARAM_COPY_WARPS, 4) == _lib.ARG
     assert L.cb_set_param(_lib.PARAM_COPY_UNITS, 3) == _lib.ARG
     assert L.cb_set_param(_lib.PARAM_CHAIN_TILE, 8192) == _lib.OK

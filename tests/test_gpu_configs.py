@@ -107,3 +107,20 @@ def test_shaped_workloads_batched(shaped):
         assert _np(t.offset).tolist() == vo.tolist(), name
         assert _np(t.length).tolist() == vl.tolist(), name
         assert _np(t.value).tolist() == iv.tolist(), name
+
+
+@pytest.mark.parametrize("tile", [2048, 8192, 65536])
+def test_chain_tiles_give_the_oracle_offsets(shaped, tile):
+    """The record chain at each tile size (a tile walked by a warp through 8 KB windows) gives the
+    oracle's record offsets and the same columns."""
+    from cubam_b200 import _lib
+
+    path, ref = shaped
+    comp = batch.load_compressed(path)
+    assert _lib.lib.cb_set_param(_lib.PARAM_CHAIN_TILE, tile) == 0
+    try:
+        d = batch.decode_resident(comp, cubam_b200.BamHeader.read(path), tags=())
+    finally:
+        _lib.lib.cb_set_param(_lib.PARAM_CHAIN_TILE, -1)
+    assert _np(d.offset).tolist() == ref.offset.tolist()
+    assert _np(d.columns["pos"]).tolist() == ref.columns["pos"].tolist()
