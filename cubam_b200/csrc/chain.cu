@@ -130,7 +130,14 @@ template <class A> __device__ bool is_record_at(const A& b, long long n, long lo
     if (32LL + lrn + 4LL * ncig + (lseq + 1) / 2 + lseq > (long long)bs) return false;
     const long long nm = o + 36;
     if (b.u8(nm + lrn - 1) != 0) return false;
-    for (uint32_t i = 0; i + 1 < lrn; i++) {
+    // the name's characters (all but its NUL): each in 33..126 and not '@', four at a time while a
+    // word holds only name characters, then one at a time (no byte past the name is read)
+    uint32_t i = 0;
+    for (; i + 4 < lrn; i += 4) {
+        const uint32_t x = b.u32(nm + i);
+        if (__vcmpltu4(x, 0x21212121u) | __vcmpgtu4(x, 0x7E7E7E7Eu) | __vcmpeq4(x, 0x40404040u)) return false;
+    }
+    for (; i + 1 < lrn; i++) {
         const uint32_t c = b.u8(nm + i);
         if (c < 33 || c > 126 || c == '@') return false;
     }
@@ -208,20 +215,28 @@ __global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b,
                 int m = 0;
                 bool stop = false;
                 if (lane == 0) {
-                    while (o < te && (o + HEAD <= hi || hi >= n)) {
-                        list[m++] = (uint16_t)(o - ts);
-                        uint32_t bs = 0;
-                        if (o + 4 <= hi) {  // block_size from the window: byte x of the data is sb[x - r0]
-                            const long long q = o - r0;
-                            const uint32_t* wd = reinterpret_cast<const uint32_t*>(sb + (q & ~3LL));
-                            bs = __funnelshift_r(wd[0], wd[1], (unsigned)(q & 3) * 8);
-                        }
-                        if (o + 36 > n || bs < 33 || bs > (1u << 22) || o + 4 + (long long)bs > n) {
+                    // in 32-bit offsets from the window start r0: x while x <= xmax (before the tile's
+                    // end, and the header inside the window unless the window reaches the data's end)
+                    const int wlen = (int)(hi - r0);
+                    const int xmax = (int)(min(te - 1, hi >= n ? te - 1 : hi - HEAD) - r0);
+                    const int nr = (int)min(n - r0, (long long)(1 << 30));  // the data's end (past 2^30: never near)
+                    const int base = (int)(r0 - ts);
+                    int x = (int)(o - r0);
+                    while (x <= xmax) {
+                        list[m++] = (uint16_t)(x + base);
+                        if (x + 4 > wlen) {  // at the data's end: not a record
                             stop = true;
                             break;
                         }
-                        o += 4 + (long long)bs;
+                        const uint32_t* wd = reinterpret_cast<const uint32_t*>(sb + (x & ~3));
+                        const uint32_t bs = __funnelshift_r(wd[0], wd[1], (unsigned)(x & 3) * 8);
+                        if (bs - 33u > (1u << 22) - 33u || x + 36 > nr || x + 4 + (int)bs > nr) {
+                            stop = true;
+                            break;
+                        }
+                        x += 4 + (int)bs;
                     }
+                    o = r0 + x;
                 }
                 m = __shfl_sync(FULL, m, 0);
                 o = __shfl_sync(FULL, o, 0);

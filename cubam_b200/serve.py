@@ -467,9 +467,12 @@ class Server:
         n_jobs = sum(len(x) for x in rows)
         summ = scratch.get("isumm", ctypes_sizeof(_lib.InflateSummary))
         if n_jobs:
-            host = torch.from_numpy(np.concatenate(rows)).pin_memory()
-            jobs = scratch.get("jobs", host.numel() * 8)
-            jobs[: host.numel() * 8].view(torch.int64).copy_(host.view(-1), non_blocking=True)
+            table = np.concatenate(rows)
+            nb = table.nbytes
+            host = scratch.host("jobs_host", nb)  # pinned, reused: the step that last used it is done
+            host[:nb].numpy()[:] = table.view(np.uint8).reshape(-1)
+            jobs = scratch.get("jobs", nb)
+            jobs[:nb].copy_(host[:nb], non_blocking=True)
             out_bytes = int(sum(int((x[:, 2] >> 32).sum()) for x in rows))  # sum of ISIZE (high half of word 2)
             qws = scratch.get("queue", inflate_workspace_bytes(n_jobs, out_bytes))
             launch_inflate(jobs.data_ptr(), n_jobs, self.pool.data_ptr(), out_bytes, self.check_crc, summ.data_ptr(),
