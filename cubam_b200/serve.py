@@ -354,7 +354,7 @@ class Server:
     way it finishes with ``status`` CB_ERR_TIMEOUT, ``error`` a TimeoutError and no result.
     """
 
-    def __init__(self, files: list[ResidentFile], budget_bytes: int = 40 << 30, step_bytes: int = 320 << 20,
+    def __init__(self, files: list[ResidentFile], budget_bytes: int = 40 << 30, step_bytes: int = 1 << 30,
                  slice_bytes: int = 48 << 20, tags=("CB", "UB", "GN"), check_crc: bool = True,
                  pool_frac: float = 0.7, short_step_bytes: int = 128 << 20, small_bytes: int = 8 << 20,
                  request_timeout: float | None = None):
