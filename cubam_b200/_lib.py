@@ -19,7 +19,7 @@ LIB_PATH = _build.LIB
 OK, TRUNCATED, NO_CHAIN, CORRUPT_BLOCK, INFLATE, CRC, TOO_MANY, CAPACITY, CUDA, ARG, TIMEOUT = range(11)
 #: launch parameters (cb_set_param / cb_get_param)
 (PARAM_CHAIN_TILE, PARAM_INFLATE_FORM, PARAM_DECODE_ROOT, PARAM_COPY_WARPS, PARAM_DECODE_STEPS, PARAM_DECODE_PREFETCH,
- PARAM_SPLIT_MIN_JOBS, PARAM_COPY_UNITS) = range(1, 9)
+ PARAM_SPLIT_MIN_JOBS, PARAM_COPY_UNITS, PARAM_DECODE_PIPELINE) = range(1, 10)
 
 
 class MemberJob(ctypes.Structure):

@@ -36,8 +36,9 @@ constexpr Param kParams[] = {
     {CB_PARAM_COPY_WARPS, 2, 24, 12},
     {CB_PARAM_DECODE_STEPS, 1, 64, 16},
     {CB_PARAM_DECODE_PREFETCH, 0, 16, 4},
-    {CB_PARAM_SPLIT_MIN_JOBS, 0, 1LL << 40, 30000},
+    {CB_PARAM_SPLIT_MIN_JOBS, 0, 1LL << 40, 8192},
     {CB_PARAM_COPY_UNITS, 1, 4, 2},
+    {CB_PARAM_DECODE_PIPELINE, 0, 2, 1},
 };
 constexpr int kNParams = sizeof(kParams) / sizeof(kParams[0]);
 std::atomic<int64_t> g_param[kNParams] = {};

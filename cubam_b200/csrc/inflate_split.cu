@@ -35,6 +35,8 @@
 // bounded per member; every shared-memory index is masked or checked; arena and output writes
 // stay within the member's slot and output range.
 
+#include <mutex>
+
 #include "common.cuh"
 #include "crc.cuh"
 
@@ -325,16 +327,17 @@ template <class C>
 __global__ void __launch_bounds__(C::WARPS * 32)
     k_decode(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
              uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes,
-             int steps, uint32_t ahead) {
+             int steps, uint32_t ahead, long long j0, long long j1, int qi) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     typename C::CtaSmem& S = *reinterpret_cast<typename C::CtaSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     typename C::WarpSmem& W = S.w[warp];
-    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws);
+    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + qi;  // this launch's counter
     uint32_t* per_job = reinterpret_cast<uint32_t*>(ws + WS_HEAD);  // (units, status, slot lo, slot hi) per job
     uint8_t* arena = ws + arena_offset(n_jobs);
     long long n = n_jobs;
     if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
+    n = min(n, j1);  // this launch's jobs: [j0, j1)
 
     uint8_t* const my_base = W.lane[lane];
     const uint16_t* my_lit = reinterpret_cast<const uint16_t*>(my_base + C::LIT);
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             if (lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(idle));
             base = __shfl_sync(FULL, base, leader);
             if (st == S_IDLE) {
-                j = (long long)base + __popc(idle & ((1u << lane) - 1u));
+                j = j0 + (long long)base + __popc(idle & ((1u << lane) - 1u));
                 if (j >= n) {
                     st = S_DONE;
                 } else {
@@ -765,7 +768,8 @@ __device__ __noinline__ uint32_t finish_crc(uint32_t col, uint32_t isize) {
 template <class C>
 __global__ void __launch_bounds__(C::WARPS * 32)
     k_copy(const cb_member_job* __restrict__ jobs, int64_t n_jobs, const int64_t* __restrict__ d_n_jobs,
-           uint8_t* out_base, int check_crc, uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws) {
+           uint8_t* out_base, int check_crc, uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws,
+           long long j0, long long j1, int qi) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     typename C::CtaSmem& S = *reinterpret_cast<typename C::CtaSmem*>(smem_raw);
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
@@ -778,17 +782,18 @@ __global__ void __launch_bounds__(C::WARPS * 32)
     uint8_t* ring = S.ring[warp];
     uint32_t* tokw = S.tok[warp];
     const uint32_t incl = lane == 31 ? 0xFFFFFFFFu : (2u << lane) - 1u;  // lanes 0..lane
-    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + 1;
+    unsigned long long* queue = reinterpret_cast<unsigned long long*>(ws) + qi;  // this launch's counter
     const uint32_t* per_job = reinterpret_cast<const uint32_t*>(ws + WS_HEAD);
     const uint8_t* arena = ws + arena_offset(n_jobs);
     long long n = n_jobs;
     if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
+    n = min(n, j1);  // this launch's jobs: [j0, j1)
     const bool crc = check_crc != 0;
 
     for (;;) {
         unsigned long long jj = 0;
         if (lane == 0) jj = atomicAdd(queue, 1ull);
-        const long long j = (long long)__shfl_sync(FULL, jj, 0);
+        const long long j = j0 + (long long)__shfl_sync(FULL, jj, 0);
         if (j >= n) break;
         if (per_job[4 * j + 1] != CB_OK) continue;  // k_decode reported it
         const cb_member_job job = jobs[j];
@@ -955,8 +960,7 @@ __global__ void k_split_init(cb_inflate_summary* summary, unsigned long long* qu
     summary->reserved = 0;
     summary->n_bad = 0;
     summary->first_bad = INT64_MAX;
-    queue[0] = 0;
-    queue[1] = 0;
+    for (int q = 0; q < 4; q++) queue[q] = 0;  // decode and copy counters of up to two job ranges
 }
 
 __global__ void k_split_finish(cb_inflate_summary* summary) {
@@ -991,34 +995,90 @@ int occupancy(int (&cache)[MAX_DEVICES], K kernel, int threads, size_t smem) {
 
 int fail_occ(int o) { return cb_set_error(o == -1 ? cudaErrorInvalidDevice : (cudaError_t)(-o)); }
 
+// One launch's jobs: [j0, j1) of the table, and its queue counters (decode at qd, copy at qd + 1).
+struct Range {
+    long long j0, j1;
+    int qd;
+};
+
 template <class D>
 int launch_decode(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint32_t* job_status,
-                  cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes, cudaStream_t s) {
+                  cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes, Range r, cudaStream_t s) {
     static int cache[MAX_DEVICES];
     const size_t smem = sizeof(typename D::CtaSmem);
     const int o = occupancy(cache, split::k_decode<D>, D::WARPS * 32, smem);
     if (o <= 0) return fail_occ(o);
     long long grid = (long long)cb_device_sm_count() * o;
-    const long long by_work = (n_jobs + 32 * D::WARPS - 1) / (32 * D::WARPS);
+    const long long by_work = (r.j1 - r.j0 + 32 * D::WARPS - 1) / (32 * D::WARPS);
     if (!d_n_jobs && by_work < grid) grid = by_work;
     split::k_decode<D><<<(unsigned)(grid < 1 ? 1 : grid), D::WARPS * 32, smem, s>>>(
         jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, (int)cb_param(CB_PARAM_DECODE_STEPS),
-        (uint32_t)cb_param(CB_PARAM_DECODE_PREFETCH));
+        (uint32_t)cb_param(CB_PARAM_DECODE_PREFETCH), r.j0, r.j1, r.qd);
     return CB_OK;
 }
 
 template <class C>
 int launch_copy(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
-                uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, cudaStream_t s) {
+                uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, Range r, cudaStream_t s) {
     static int cache[MAX_DEVICES];
     const size_t smem = sizeof(typename C::CtaSmem);
     const int o = occupancy(cache, split::k_copy<C>, C::WARPS * 32, smem);
     if (o <= 0) return fail_occ(o);
     long long grid = (long long)cb_device_sm_count() * o;
-    const long long by_work = (n_jobs + C::WARPS - 1) / C::WARPS;
+    const long long by_work = (r.j1 - r.j0 + C::WARPS - 1) / C::WARPS;
     if (!d_n_jobs && by_work < grid) grid = by_work;
     split::k_copy<C><<<(unsigned)(grid < 1 ? 1 : grid), C::WARPS * 32, smem, s>>>(
-        jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws);
+        jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, r.j0, r.j1, r.qd + 1);
+    return CB_OK;
+}
+
+int decode_range(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint32_t* job_status,
+                 cb_inflate_summary* summary, uint8_t* ws, unsigned long long arena_bytes, Range r, cudaStream_t s) {
+    const int rb = (int)cb_param(CB_PARAM_DECODE_ROOT);
+    if (rb == 8)
+        return launch_decode<split::DecCfg<8, 6, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, r, s);
+    if (rb == 7)
+        return launch_decode<split::DecCfg<7, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, r, s);
+    return launch_decode<split::DecCfg<6, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, r, s);
+}
+
+int copy_range(const cb_member_job* jobs, int64_t n_jobs, const int64_t* d_n_jobs, uint8_t* out_base, int check_crc,
+               uint32_t* job_status, cb_inflate_summary* summary, uint8_t* ws, Range r, cudaStream_t s) {
+    const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
+    const int units = (int)cb_param(CB_PARAM_COPY_UNITS);
+#define CB_COPY(W, R, UPL) \
+    launch_copy<split::CopyCfg<W, R, UPL>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, r, s)
+    if (cw == 2) return CB_COPY(2, 16384, 1);
+    if (cw == 3) return CB_COPY(3, 16384, 1);
+    if (cw == 12) return units == 4 ? CB_COPY(12, 8192, 4) : units == 2 ? CB_COPY(12, 8192, 2) : CB_COPY(12, 8192, 1);
+    if (cw == 24) return units >= 2 ? CB_COPY(24, 4096, 2) : CB_COPY(24, 4096, 1);
+    return units == 4 ? CB_COPY(6, 16384, 4) : units == 2 ? CB_COPY(6, 16384, 2) : CB_COPY(6, 16384, 1);
+#undef CB_COPY
+}
+
+// Two side streams per device for the pipelined form, and the events that join them to the caller's
+// stream; the mutex keeps each call's records and waits together (a wait takes the event's state
+// when it is called), so calls from several host threads may share them.
+struct Side {
+    cudaStream_t x = nullptr, y = nullptr;
+    cudaEvent_t start = nullptr, done_x = nullptr, done_y = nullptr;
+    bool ready = false;
+};
+Side g_side[MAX_DEVICES];
+std::mutex g_side_mu;
+
+int side_for(int dev, Side*& out) {
+    Side& sd = g_side[dev];
+    if (!sd.ready) {
+        cudaError_t e = cudaStreamCreateWithFlags(&sd.x, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sd.y, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sd.start, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sd.done_x, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sd.done_y, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cb_set_error(e);
+        sd.ready = true;
+    }
+    out = &sd;
     return CB_OK;
 }
 
@@ -1039,31 +1099,46 @@ extern "C" int cb_inflate_split(const cb_member_job* jobs, int64_t n_jobs, const
     split::k_split_init<<<1, 1, 0, s>>>(summary, reinterpret_cast<unsigned long long*>(ws));
     if (n_jobs > 0) {
         split::k_slots<<<1, split::SLOT_NT, 0, s>>>(jobs, n_jobs, d_n_jobs, ws);
-        const int rb = (int)cb_param(CB_PARAM_DECODE_ROOT);
-        int rc;
-        if (rb == 8)
-            rc = launch_decode<split::DecCfg<8, 6, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
-        else if (rb == 7)
-            rc = launch_decode<split::DecCfg<7, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
-        else
-            rc = launch_decode<split::DecCfg<6, 5, 1>>(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, s);
-        if (rc != CB_OK) return rc;
-        const int cw = (int)cb_param(CB_PARAM_COPY_WARPS);
-        const int units = (int)cb_param(CB_PARAM_COPY_UNITS);
-#define CB_COPY(W, R, UPL) \
-    launch_copy<split::CopyCfg<W, R, UPL>>(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, s)
-        if (cw == 2)
-            rc = CB_COPY(2, 16384, 1);
-        else if (cw == 3)
-            rc = CB_COPY(3, 16384, 1);
-        else if (cw == 12)
-            rc = units == 4 ? CB_COPY(12, 8192, 4) : units == 2 ? CB_COPY(12, 8192, 2) : CB_COPY(12, 8192, 1);
-        else if (cw == 24)
-            rc = units >= 2 ? CB_COPY(24, 4096, 2) : CB_COPY(24, 4096, 1);
-        else
-            rc = units == 4 ? CB_COPY(6, 16384, 4) : units == 2 ? CB_COPY(6, 16384, 2) : CB_COPY(6, 16384, 1);
-#undef CB_COPY
-        if (rc != CB_OK) return rc;
+        // Pipelined: the jobs in two ranges, each decoded and then copied on its own stream, so that
+        // the second range's decode and the first range's copy take the GPU while the other decode
+        // runs out of members (one member per lane leaves lanes idle at its end).  Only with the job
+        // count known on the host.
+        const long long pipe = cb_param(CB_PARAM_DECODE_PIPELINE);
+        const bool two = !d_n_jobs && n_jobs >= 2 && (pipe == 2 || (pipe == 1 && n_jobs >= 65536));
+        int rc = CB_OK;
+        if (!two) {
+            const Range all{0, n_jobs, 0};
+            rc = decode_range(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, all, s);
+            if (rc == CB_OK) rc = copy_range(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, all, s);
+            if (rc != CB_OK) return rc;
+        } else {
+            int dev = 0;
+            cudaError_t e = cudaGetDevice(&dev);
+            if (e != cudaSuccess) return cb_set_error(e);
+            if (dev < 0 || dev >= MAX_DEVICES) return CB_ERR_ARG;
+            std::lock_guard<std::mutex> lock(g_side_mu);
+            Side* sd = nullptr;
+            if ((rc = side_for(dev, sd)) != CB_OK) return rc;
+            const long long cut = n_jobs - n_jobs / 4;  // three quarters first
+            const Range ra{0, cut, 0}, rb{cut, n_jobs, 2};
+            e = cudaEventRecord(sd->start, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(sd->x, sd->start, 0);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(sd->y, sd->start, 0);
+            if (e != cudaSuccess) return cb_set_error(e);
+            rc = decode_range(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, ra, sd->x);
+            if (rc == CB_OK) rc = decode_range(jobs, n_jobs, d_n_jobs, job_status, summary, ws, arena_bytes, rb, sd->y);
+            if (rc == CB_OK)
+                rc = copy_range(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, ra, sd->x);
+            if (rc == CB_OK)
+                rc = copy_range(jobs, n_jobs, d_n_jobs, out_base, check_crc, job_status, summary, ws, rb, sd->y);
+            // join both side streams back to the caller's stream whatever happened above
+            e = cudaEventRecord(sd->done_x, sd->x);
+            if (e == cudaSuccess) e = cudaEventRecord(sd->done_y, sd->y);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, sd->done_x, 0);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, sd->done_y, 0);
+            if (rc != CB_OK) return rc;
+            if (e != cudaSuccess) return cb_set_error(e);
+        }
     }
     split::k_split_finish<<<1, 1, 0, s>>>(summary);
     return cb_set_error(cudaGetLastError());

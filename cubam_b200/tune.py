@@ -36,12 +36,13 @@ CANDIDATES = {
     "copy_units": (_lib.PARAM_COPY_UNITS, (1, 2, 4)),
     "decode_steps": (_lib.PARAM_DECODE_STEPS, (8, 16, 32)),
     "decode_prefetch": (_lib.PARAM_DECODE_PREFETCH, (0, 4, 8)),
+    "decode_pipeline": (_lib.PARAM_DECODE_PIPELINE, (0, 2)),
     "chain_tile": (_lib.PARAM_CHAIN_TILE, (0, 16384, 32768)),
 }
 #: the stage each parameter is timed on (StageEvents names)
 STAGE = {"chain_tile": "chained"}
 #: form-3 parameters are tuned only when form 3 wins
-FORM3 = ("decode_root", "copy_warps", "copy_units", "decode_steps", "decode_prefetch")
+FORM3 = ("decode_root", "copy_warps", "copy_units", "decode_steps", "decode_prefetch", "decode_pipeline")
 
 
 def cache_path() -> Path:

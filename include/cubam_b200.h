@@ -101,10 +101,15 @@ int cb_device_sm_count(void);
  *                          each lane's position: 0-16, 0 = none (4)
  *   CB_PARAM_SPLIT_MIN_JOBS   with CB_PARAM_INFLATE_FORM 3, form 0 runs form 1 for calls of fewer jobs
  *                          (form 3 decodes one member per lane, so it needs many members to fill the GPU):
- *                          0 or more (30000)
+ *                          0 or more (8192; on 15,456 GEX members form 3 took 16.7 ms, form 1 22.0)
  *   CB_PARAM_COPY_UNITS    DEFLATE units each lane of form 3's copy kernel takes per group: 1 (groups of
  *                          32 units), 2 (64; with 6, 12 or 24 copy warps) or 4 (128; with 6 or 12 copy
  *                          warps, else 2) (2)
+ *   CB_PARAM_DECODE_PIPELINE  form 3 in two job ranges, each decoded and then copied on its own stream
+ *                          (side streams joined back to the caller's by events), so that one range's
+ *                          decode and the other's copy fill the lanes a decode leaves idle at its end:
+ *                          0 never, 1 from 65,536 jobs, 2 always; only with the job count given on the
+ *                          host (d_n_jobs NULL) (1)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
@@ -115,7 +120,8 @@ enum {
     CB_PARAM_DECODE_STEPS = 5,
     CB_PARAM_DECODE_PREFETCH = 6,
     CB_PARAM_SPLIT_MIN_JOBS = 7,
-    CB_PARAM_COPY_UNITS = 8
+    CB_PARAM_COPY_UNITS = 8,
+    CB_PARAM_DECODE_PIPELINE = 9
 };
 int cb_set_param(int key, int64_t value);
 int64_t cb_get_param(int key);

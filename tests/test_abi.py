@@ -66,5 +66,6 @@ def test_launch_parameters_are_checked_and_restored():
     assert L.cb_get_param(_lib.PARAM_CHAIN_TILE) == 0
     for key, default in ((_lib.PARAM_INFLATE_FORM, 3), (_lib.PARAM_DECODE_ROOT, 7), (_lib.PARAM_COPY_WARPS, 12),
                          (_lib.PARAM_DECODE_STEPS, 16), (_lib.PARAM_DECODE_PREFETCH, 4),
-                         (_lib.PARAM_SPLIT_MIN_JOBS, 30000), (_lib.PARAM_COPY_UNITS, 2)):
+                         (_lib.PARAM_SPLIT_MIN_JOBS, 8192), (_lib.PARAM_COPY_UNITS, 2),
+                         (_lib.PARAM_DECODE_PIPELINE, 1)):
         assert L.cb_get_param(key) == default

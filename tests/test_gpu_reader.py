@@ -171,9 +171,11 @@ def _payloads(seed: int):
 
 
 # one member per warp, one member per lane, decode per lane + copy per warp (form 3 also with the copy
-# kernel's groups of 32 and 128 units, 64 at 24 warps, and with the decoder's 8-bit root tables)
-FORMS = [1, 2, 3, "3/u1", "3/u4", "3/u2/w24", "3/r8"]
-_FORM_PARAMS = {"u": G._lib.PARAM_COPY_UNITS, "w": G._lib.PARAM_COPY_WARPS, "r": G._lib.PARAM_DECODE_ROOT}
+# kernel's groups of 32 and 128 units, 64 at 24 warps, with the decoder's 8-bit root tables, and with
+# the two-range pipeline always and never)
+FORMS = [1, 2, 3, "3/u1", "3/u4", "3/u2/w24", "3/r8", "3/p2", "3/p0"]
+_FORM_PARAMS = {"u": G._lib.PARAM_COPY_UNITS, "w": G._lib.PARAM_COPY_WARPS, "r": G._lib.PARAM_DECODE_ROOT,
+                "p": G._lib.PARAM_DECODE_PIPELINE}
 
 
 class _Form:
