@@ -899,6 +899,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
             __syncwarp();
             uint32_t before = 0;  // tokens that start before this round
             uint32_t ri = 0;
+#pragma unroll 2
             for (uint32_t r0 = 0; r0 < glen; r0 += 32, ri++) {
                 const uint32_t rel = r0 + lane;
                 // the token of byte rel: tokens starting in this round set bits of a mask; the byte's
