@@ -109,7 +109,8 @@ int cb_device_sm_count(void);
  *                          (side streams joined back to the caller's by events), so that one range's
  *                          decode and the other's copy fill the lanes a decode leaves idle at its end:
  *                          0 never, 1 from 65,536 jobs, 2 always; only with the job count given on the
- *                          host (d_n_jobs NULL) (1)
+ *                          host (d_n_jobs NULL).  The side streams and events are created by the first
+ *                          pipelined call on a device, which should come before any stream capture (1)
  * cb_set_param(key, -1) restores the default; an unknown key or a value out of range is CB_ERR_ARG.
  * cb_get_param returns the current value, -1 for an unknown key. */
 enum {
