@@ -52,7 +52,7 @@ FALLBACK_HBM = 6650.0
 #: 4M-record GEX file (1,008,824,685 inflated bytes); the bench scales them by its inflated bytes
 TRAFFIC_PER_BYTE = {"k_inflate_lanes": (6.916637e9 + 1.003612e9) / 1.008824685e9,
                     "k_inflate_warp": (1.593613e9 + 1.004537e9) / 1.008824685e9,
-                    "k_decode + k_copy": (0.41414656e9 + 0.754893568e9 + 1.479409e9 + 0.955981568e9) / 1.008824685e9}
+                    "k_decode + k_copy": (0.414233344e9 + 0.754765312e9 + 1.45392e9 + 0.958392832e9) / 1.008824685e9}
 
 
 def parse():
