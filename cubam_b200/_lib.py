@@ -89,7 +89,7 @@ _SIGNATURES = {
     "cb_decode_fixed": (c_int, [P, P, I64] + [P] * 11 + [P]),
     "cb_decode_records": (c_int, [P, P, I64] + [P] * 13 + [P]),
     "cb_find_tags": (c_int, [P, P, I64, c_char_p, c_int32, P, P, P, P, P]),
-    "cb_decode_columns": (c_int, [P, P, I64] + [P] * 13 + [c_char_p, c_int32, P, P, P, P, P]),
+    "cb_decode_columns": (c_int, [P, P, I64] + [P] * 15 + [c_char_p, c_int32, P, P, P, P, P]),
     "cb_name_hash": (c_int, [P, P, I64, P, P]),
     "cb_hash_spans": (c_int, [P, P, P, I64, P, P]),
     "cb_pack_acgt": (c_int, [P, P, P, I64, P, P, P]),

@@ -355,22 +355,26 @@ class RecordBatch:
 
     @classmethod
     def decode(cls, data: torch.Tensor, offset: torch.Tensor, header: BamHeader, derived: bool = False) -> RecordBatch:
-        """Fixed columns of the records; with ``derived`` also their aligned lengths and read-name hashes,
-        in the same pass over the record bytes (then :meth:`aligned_length` and :meth:`name_hash` return
-        them without reading the records again)."""
+        """Fixed columns of the records; with ``derived`` also their aligned lengths, read-name hashes
+        and aligned-block counts (both modes of :meth:`blocks`), in the same pass over the record bytes
+        (then :meth:`aligned_length` and :meth:`name_hash` return them without reading the records
+        again, and :meth:`blocks` runs only its writing pass)."""
         n = int(offset.numel())
         cols = {k: torch.empty(n, dtype=t, device="cuda") for k, t in _TYPES.items()}
         extra = {}
         if derived:
             extra = {"aligned_length": torch.empty(n, dtype=torch.int32, device="cuda"),
-                     "name_hash": torch.empty(n, dtype=torch.uint64, device="cuda")}
+                     "name_hash": torch.empty(n, dtype=torch.uint64, device="cuda"),
+                     "n_blocks": torch.empty(n, dtype=torch.int32, device="cuda"),
+                     "n_blocks_split": torch.empty(n, dtype=torch.int32, device="cuda")}
         if n:
             if derived:
-                rc = _lib.lib.cb_decode_records(data.data_ptr(), offset.data_ptr(), n,
+                rc = _lib.lib.cb_decode_columns(data.data_ptr(), offset.data_ptr(), n,
                                                 *(cols[k].data_ptr() for k in FIELDS),
-                                                extra["aligned_length"].data_ptr(), extra["name_hash"].data_ptr(),
-                                                stream_ptr())
-                _lib.check(rc, "cb_decode_records")
+                                                *(extra[k].data_ptr() for k in ("aligned_length", "name_hash",
+                                                                                "n_blocks", "n_blocks_split")),
+                                                b"", 0, None, None, None, None, stream_ptr())
+                _lib.check(rc, "cb_decode_columns")
             else:
                 rc = _lib.lib.cb_decode_fixed(data.data_ptr(), offset.data_ptr(), n,
                                               *(cols[k].data_ptr() for k in FIELDS), stream_ptr())
@@ -452,11 +456,16 @@ class RecordBatch:
     def blocks(self, split_deletions: bool = False):
         """Aligned blocks of the reads: ``(rec, start, end)``, one row per block, in read order."""
         n = len(self)
-        cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
         off = self.offset.contiguous()
-        if n:
-            _lib.check(_lib.lib.cb_blocks(self.data.data_ptr(), off.data_ptr(), n, int(split_deletions), 0, None,
-                                          cnt.data_ptr(), None, None, None, stream_ptr()), "cb_blocks")
+        d = self.__dict__.get("_derived")
+        key = "n_blocks_split" if split_deletions else "n_blocks"
+        if d and key in d:  # counted by the record pass
+            cnt = d[key].contiguous()
+        else:
+            cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+            if n:
+                _lib.check(_lib.lib.cb_blocks(self.data.data_ptr(), off.data_ptr(), n, int(split_deletions), 0,
+                                              None, cnt.data_ptr(), None, None, None, stream_ptr()), "cb_blocks")
         first = torch.zeros(n, dtype=torch.int64, device="cuda")
         if n > 1:
             first[1:] = torch.cumsum(cnt[:-1], 0, dtype=torch.int64)

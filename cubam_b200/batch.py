@@ -214,7 +214,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
             rc = _lib.lib.cb_decode_columns(
                 data.data_ptr(), off.data_ptr(), nrec, *(cols[f].data_ptr() for f in FIELDS),
                 cols["aligned_length"].data_ptr() if derived else None, cols["name_hash"].data_ptr() if derived else None,
-                "".join(tags).encode(), k, *((a.data_ptr() for a in arrs) if k else (None,) * 4), stream_ptr())
+                None, None, "".join(tags).encode(), k, *((a.data_ptr() for a in arrs) if k else (None,) * 4), stream_ptr())
             _lib.check(rc, "cb_decode_columns")
             if k:
                 view = _View(data, off)
@@ -373,7 +373,7 @@ class BatchPlan:
             cols = res.columns
             k = len(self.tags) if arrs is not None else 0
             rc = _lib.lib.cb_decode_columns(res.data.data_ptr(), res.offset.data_ptr(), nrec,
-                                            *(cols[f].data_ptr() for f in FIELDS), None, None,
+                                            *(cols[f].data_ptr() for f in FIELDS), None, None, None, None,
                                             "".join(self.tags).encode(), k,
                                             *((a.data_ptr() for a in arrs) if k else (None,) * 4), s)
             _lib.check(rc, "cb_decode_columns")

@@ -169,7 +169,8 @@ int launch_records(cb_batch* b, cudaStream_t s) {
         if (!f.n_records) continue;
         const int rc = cb_decode_columns(b->out + f.out_base + f.header_bytes, f.offsets, f.n_records, f.ref, f.pos,
                                          f.end, f.mapq, f.flag, f.nref, f.npos, f.tlen, f.l_seq, f.clip_left,
-                                         f.clip_right, nullptr, nullptr, b->tags, b->k, f.tag_type, f.tag_voff,
+                                         f.clip_right, nullptr, nullptr, nullptr, nullptr, b->tags, b->k, f.tag_type,
+                                         f.tag_voff,
                                          f.tag_vlen, f.tag_value, s);
         if (rc != CB_OK) return rc;
     }

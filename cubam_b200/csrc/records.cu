@@ -40,6 +40,28 @@ struct Cols {
     uint16_t *clip_left, *clip_right;
     int32_t* aligned;
     uint64_t* name_hash;
+    int32_t* nblk;        // aligned blocks per read, deletions inside a block (as blocks(split_deletions=0))
+    int32_t* nblk_split;  // the same with deletions splitting blocks
+};
+
+// Aligned blocks of one read in the two modes of blocks() (src/cubam/_kernels.py:408-437): a block
+// ends at an N (and, splitting, at a D) and is counted when it covers a reference base.
+struct BlockCount {
+    uint32_t x = 0, s = 0;
+    int k = 0;
+    __device__ __forceinline__ void start(uint32_t pos) { x = s = pos; }
+    __device__ __forceinline__ void op(uint32_t op, uint32_t l, bool split) {
+        const bool aligned = op == 0 || op == 7 || op == 8 || (op == 2 && !split);
+        const bool gap = op == 3 || (op == 2 && split);
+        if (aligned) {
+            x += l;
+        } else if (gap) {
+            if ((int)x > (int)s) k++;
+            x += l;
+            s = x;
+        }
+    }
+    __device__ __forceinline__ int end() const { return k + ((int)x > (int)s ? 1 : 0); }
 };
 
 struct TagNames {
@@ -82,16 +104,22 @@ __device__ __forceinline__ void parse_record(const Win& w, long long o, long lon
     const uint32_t w12 = w.u32(o + 12), w16 = w.u32(o + 16);
     const uint32_t lrn = w12 & 255, ncig = w16 & 0xffff;
     const uint32_t lseq = w.u32(o + 20);
-    if (cols) {
+    const bool blocks = c.nblk || c.nblk_split;
+    if (cols || blocks) {
         const int p = (int)w.u32(o + 8);
-        c.ref[i] = (int)w.u32(o + 4);
-        c.pos[i] = p;
-        c.mapq[i] = (uint8_t)(w12 >> 8);
-        c.flag[i] = (uint16_t)(w16 >> 16);
-        c.nref[i] = (int)w.u32(o + 24);
-        c.npos[i] = (int)w.u32(o + 28);
-        c.tlen[i] = (int)w.u32(o + 32);
-        c.l_seq[i] = (int)lseq;
+        BlockCount b0, b1;
+        b0.start((uint32_t)p);
+        b1.start((uint32_t)p);
+        if (cols) {
+            c.ref[i] = (int)w.u32(o + 4);
+            c.pos[i] = p;
+            c.mapq[i] = (uint8_t)(w12 >> 8);
+            c.flag[i] = (uint16_t)(w16 >> 16);
+            c.nref[i] = (int)w.u32(o + 24);
+            c.npos[i] = (int)w.u32(o + 28);
+            c.tlen[i] = (int)w.u32(o + 32);
+            c.l_seq[i] = (int)lseq;
+        }
         const long long cg = o + 36 + lrn;
         long long rlen = 0;
         uint32_t cl = 0, cr = 0, al = 0;
@@ -103,11 +131,19 @@ __device__ __forceinline__ void parse_record(const Win& w, long long o, long lon
                 if (q == 0) cl = len;
                 else cr = len;
             }
+            if (blocks) {
+                b0.op(op, len, false);
+                b1.op(op, len, true);
+            }
         }
-        c.end[i] = p + (int)rlen;
-        c.clip_left[i] = (uint16_t)(cl > 65535 ? 65535 : cl);
-        c.clip_right[i] = (uint16_t)(cr > 65535 ? 65535 : cr);
+        if (cols) {
+            c.end[i] = p + (int)rlen;
+            c.clip_left[i] = (uint16_t)(cl > 65535 ? 65535 : cl);
+            c.clip_right[i] = (uint16_t)(cr > 65535 ? 65535 : cr);
+        }
         if (c.aligned) c.aligned[i] = (int32_t)al;
+        if (c.nblk) c.nblk[i] = b0.end();
+        if (c.nblk_split) c.nblk_split[i] = b1.end();
     } else if (c.aligned) {
         const long long cg = o + 36 + lrn;
         uint32_t al = 0;
@@ -476,10 +512,12 @@ static int launch_records(const uint8_t* data, const int64_t* offsets, int64_t n
 extern "C" int cb_decode_columns(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
                                  int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos,
                                  int32_t* tlen, int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right,
-                                 int32_t* aligned_length, uint64_t* name_hash, const char* names, int32_t k,
-                                 uint8_t* type, int64_t* voff, int32_t* vlen, int64_t* value, void* stream) {
-    const rec::Cols c{ref, pos, end, mapq, flag, nref, npos, tlen, l_seq, clip_left, clip_right, aligned_length,
-                      name_hash};
+                                 int32_t* aligned_length, uint64_t* name_hash, int32_t* n_blocks,
+                                 int32_t* n_blocks_split, const char* names, int32_t k, uint8_t* type,
+                                 int64_t* voff, int32_t* vlen, int64_t* value, void* stream) {
+    const rec::Cols c{ref,       pos,        end,      mapq,           flag,     nref, npos,
+                      tlen,      l_seq,      clip_left, clip_right,    aligned_length, name_hash,
+                      n_blocks,  n_blocks_split};
     return launch_records(data, offsets, n, c, ref != nullptr, names, k, type, voff, vlen, value, stream);
 }
 

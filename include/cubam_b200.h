@@ -239,16 +239,18 @@ int cb_decode_records(const uint8_t* data, const int64_t* offsets, int64_t n, in
                       uint64_t* name_hash, void* stream);
 
 /* The record pass in one launch: the fixed columns (all eleven pointers, or ref == NULL for none),
- * aligned_length and name_hash (each skipped when NULL) and k <= 16 aux tags (k = 0 for none; layout
- * as cb_find_tags), from one read of each record's bytes.  A warp stages the bytes of 32 consecutive
+ * aligned_length, name_hash, n_blocks and n_blocks_split (each skipped when NULL; the last two count
+ * the aligned blocks of cb_blocks with split_del 0 and 1, fusing its counting pass,
+ * src/cubam/_kernels.py:408-437) and k <= 16 aux tags (k = 0 for none; layout as cb_find_tags), from
+ * one read of each record's bytes.  A warp stages the bytes of 32 consecutive
  * records in shared memory with coalesced loads and each lane parses one record; bytes outside the
  * staged window are read from global memory, so any offsets are accepted.  cb_decode_fixed,
  * cb_decode_records and cb_find_tags are this pass with the other outputs left out. */
 int cb_decode_columns(const uint8_t* data, const int64_t* offsets, int64_t n, int32_t* ref, int32_t* pos,
                       int32_t* end, uint8_t* mapq, uint16_t* flag, int32_t* nref, int32_t* npos, int32_t* tlen,
                       int32_t* l_seq, uint16_t* clip_left, uint16_t* clip_right, int32_t* aligned_length,
-                      uint64_t* name_hash, const char* names, int32_t k, uint8_t* type, int64_t* voff,
-                      int32_t* vlen, int64_t* value, void* stream);
+                      uint64_t* name_hash, int32_t* n_blocks, int32_t* n_blocks_split, const char* names,
+                      int32_t k, uint8_t* type, int64_t* voff, int32_t* vlen, int64_t* value, void* stream);
 
 /* ---- Tags: replaces find_tag, one launch per tag (src/cubam/_kernels.py:334-388, src/cubam/bam.py:184-208).
  * One aux walk per record finds k tags (k <= 16); `names` (host) holds 2k characters.  Output is

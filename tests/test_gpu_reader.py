@@ -342,7 +342,8 @@ def test_records_cross_members_and_chunks(tmp_path):
 
 @pytest.mark.parametrize(("name", "chunk"), [("mixed_b700.bam", 50_000), ("pairs.bam", 1 << 20)])
 def test_fused_record_pass_equals_the_separate_decoders(name, chunk):
-    """decode(derived=True) gives the aligned lengths and name hashes of the separate kernels, in one pass."""
+    """decode(derived=True) gives the aligned lengths, name hashes and aligned blocks of the separate
+    kernels, the blocks' counts from the same pass."""
     from golden_io import GOLDEN
 
     from cubam_b200.bam import RecordBatch
@@ -353,9 +354,15 @@ def test_fused_record_pass_equals_the_separate_decoders(name, chunk):
             assert torch.equal(getattr(f, k), getattr(b, k)), k
         assert torch.equal(f.aligned_length(), b.aligned_length())
         assert torch.equal(f.name_hash().view(torch.int64), b.name_hash().view(torch.int64))
+        for split in (False, True):
+            assert f.__dict__["_derived"]["n_blocks_split" if split else "n_blocks"] is not None
+            for x, y in zip(f.blocks(split), b.blocks(split)):
+                assert torch.equal(x, y), split
         idx = torch.arange(0, len(b), 3, device="cuda")
         t = f.take(idx)
         assert torch.equal(t.aligned_length(), b.take(idx).aligned_length())
+        for x, y in zip(t.blocks(True), b.take(idx).blocks(True)):
+            assert torch.equal(x, y)
 
 
 def test_too_many_member_candidates():
