@@ -116,11 +116,12 @@ __device__ __forceinline__ int reg2bin(int beg, int end) {
 }
 
 // The reference's record predicate at offset o (src/cubam/_kernels.py:250-278), on the bytes of
-// accessor A (GlobalBytes or StagedBytes).
-template <class A> __device__ bool is_record_at(const A& b, long long n, long long o, int n_ref) {
+// accessor A (GlobalBytes or StagedBytes with 64-bit offsets I, WindowBytes with 32-bit offsets from
+// its window; n is the data's end in the same offsets).
+template <class A, class I> __device__ __forceinline__ bool is_record_at(const A& b, I n, I o, int n_ref) {
     if (o < 0 || o + 36 > n) return false;
     const int bs = (int)b.u32(o);
-    if (bs < 33 || bs > (1 << 22) || o + 4 + (long long)bs > n) return false;
+    if (bs < 33 || bs > (1 << 22) || o + 4 + (I)bs > n) return false;
     const int ref = (int)b.u32(o + 4), pos = (int)b.u32(o + 8);
     const int nref = (int)b.u32(o + 24), npos = (int)b.u32(o + 28);
     if (ref < -1 || ref >= n_ref || pos < -1 || nref < -1 || nref >= n_ref || npos < -1) return false;
@@ -128,23 +129,23 @@ template <class A> __device__ bool is_record_at(const A& b, long long n, long lo
     const uint32_t lrn = w12 & 255, ncig = w16 & 0xffff, flag = w16 >> 16;
     if (lrn < 2 || flag >= 4096 || lseq > (1u << 22)) return false;
     if (32LL + lrn + 4LL * ncig + (lseq + 1) / 2 + lseq > (long long)bs) return false;
-    const long long nm = o + 36;
-    if (b.u8(nm + lrn - 1) != 0) return false;
+    const I nm = o + 36;
+    if (b.u8(nm + (I)lrn - 1) != 0) return false;
     // the name's characters (all but its NUL): each in 33..126 and not '@', four at a time while a
     // word holds only name characters, then one at a time (no byte past the name is read)
     uint32_t i = 0;
     for (; i + 4 < lrn; i += 4) {
-        const uint32_t x = b.u32(nm + i);
+        const uint32_t x = b.u32(nm + (I)i);
         if (__vcmpltu4(x, 0x21212121u) | __vcmpgtu4(x, 0x7E7E7E7Eu) | __vcmpeq4(x, 0x40404040u)) return false;
     }
     for (; i + 1 < lrn; i++) {
-        const uint32_t c = b.u8(nm + i);
+        const uint32_t c = b.u8(nm + (I)i);
         if (c < 33 || c > 126 || c == '@') return false;
     }
-    const long long cg = nm + lrn;
+    const I cg = nm + (I)lrn;
     long long rlen = 0;
-    for (uint32_t i = 0; i < ncig; i++) {
-        const uint32_t v = b.u32(cg + 4LL * i), op = v & 15;
+    for (uint32_t q = 0; q < ncig; q++) {
+        const uint32_t v = b.u32(cg + 4 * (I)q), op = v & 15;
         if (op > 8) return false;
         if (op == 0 || op == 2 || op == 3 || op == 7 || op == 8) rlen += v >> 4;
     }
@@ -156,7 +157,7 @@ template <class A> __device__ bool is_record_at(const A& b, long long n, long lo
 }
 
 __device__ __forceinline__ bool is_record(const uint8_t* b, long long n, long long o, int n_ref) {
-    return is_record_at(GlobalBytes{b}, n, o, n_ref);
+    return is_record_at<GlobalBytes, long long>(GlobalBytes{b}, n, o, n_ref);
 }
 
 __global__ void k_init(Ws w) {
@@ -186,12 +187,15 @@ __global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b,
                 hi = min(base + WIN + HALO, n);
                 r0 = stage_bytes(b, base, hi, st);
             }
-            const StagedBytes d{b, sb, r0, hi};
+            // the window's bytes by 32-bit offsets from r0 (the data's end past 2^30 is never near)
+            const WindowBytes d{b + r0, sb, (int)(hi - r0)};
+            const int nr = (int)min(n - r0, (long long)(1 << 30));
             const long long o = base + lane;
             bool ok = false;
             if (o < te && o + 4 <= n) {
-                const uint32_t bs = d.u32(o);
-                if (bs - 33u <= (1u << 22) - 33u) ok = is_record_at(d, n, o, n_ref);
+                const int x = (int)(o - r0);
+                const uint32_t bs = d.u32(x);
+                if (bs - 33u <= (1u << 22) - 33u) ok = is_record_at(d, nr, x, n_ref);
             }
             const unsigned m = __ballot_sync(FULL, ok);
             if (m) {
@@ -243,11 +247,13 @@ __global__ void __launch_bounds__(WW * 32) k_walk(const uint8_t* __restrict__ b,
                 stop = __shfl_sync(FULL, (int)stop, 0) != 0;
                 __syncwarp();
                 // the predicate on the listed records, in parallel: the count ends at the first failure
-                const StagedBytes d{b, sb, r0, hi};
+                const WindowBytes d{b + r0, sb, (int)(hi - r0)};
+                const int nr = (int)min(n - r0, (long long)(1 << 30));
+                const int xt = (int)(ts - r0);  // the tile start from the window start (may be negative)
                 int f = m;
                 for (int j0 = 0; j0 < m; j0 += 32) {
                     const int j = j0 + lane;
-                    const bool ok = j >= m || is_record_at(d, n, ts + list[j], n_ref);
+                    const bool ok = j >= m || is_record_at(d, nr, xt + (int)list[j], n_ref);
                     const unsigned bad = __ballot_sync(FULL, !ok);
                     if (bad) {
                         f = j0 + __ffs(bad) - 1;

@@ -51,6 +51,25 @@ struct StagedBytes {
     }
 };
 
+// The same staged window addressed by 32-bit offsets x from its start r0 (x >= 0): s holds bytes
+// [0, wlen), g = data + r0 reaches the rest.  For walks that stay within 2^30 bytes of r0.
+struct WindowBytes {
+    const uint8_t* g;
+    const uint8_t* s;
+    int wlen;
+    __device__ __forceinline__ uint32_t u8(int x) const { return x < wlen ? s[x] : __ldg(g + x); }
+    __device__ __forceinline__ uint32_t u16(int x) const {
+        return x + 2 <= wlen ? (uint32_t)s[x] | ((uint32_t)s[x + 1] << 8) : ld_u16(g, x);
+    }
+    __device__ __forceinline__ uint32_t u32(int x) const {
+        if (x + 4 <= wlen) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(s + (x & ~3));
+            return __funnelshift_r(w[0], w[1], (unsigned)(x & 3) * 8);
+        }
+        return ld_u32(g, x);
+    }
+};
+
 // Copy the data bytes [lo, hi) to shared memory `st` with the warp's asynchronous 16-byte copies
 // (cp.async: coalesced, all in flight at once, no registers held; the first and last 16-byte blocks
 // are copied whole, which never leaves the pages holding the range), then wait for them and sync the
