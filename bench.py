@@ -1,6 +1,7 @@
 """Benchmark of the BAM reader hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config gex|small|atac]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config gex|small|atac|uneven|serve|bai|write]
 
 One step = one decode of the whole synthetic BAM of the workload (default: the
 GEX-shaped batch, 50,000,000 single-end 91 bp records over the 25 human
@@ -17,6 +18,9 @@ fixed columns and the CB/UB/GN tags.  The metric is GB/s of decompressed
   kernels, and a D2H read of the per-step checksum, timed by the device clock.
 - ``roofline``: the inflate kernel (the dominant one): decompressed bytes per
   launch / its CUDA-event duration, against the measured HBM copy bandwidth.
+- ``serving``: the serving loop on the same file, bounded (100 requests of log-uniform
+  64 KB-512 MB compressed ranges, all at once, then Poisson at 80% of that rate):
+  p50/p95/p99 latency and throughput against the batched decode.
 - ``cpu_baseline``: the C oracle (zlib inflate + record chain + columns, all host
   cores) on a bounded prefix of the same file; ``parity`` compares the GPU's
   records, columns and tags of that prefix with the oracle's ("ok" or the first

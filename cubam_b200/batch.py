@@ -8,11 +8,12 @@ same kernels for files whose compressed bytes are already on the device:
 1. ``cb_scan_members`` runs on every file (launched back to back, one
    synchronisation for all of them) and gives each file's inflate jobs, with
    output offsets placed one file after another in one output arena;
-2. ONE ``cb_inflate`` launch inflates the members of all files: a persistent
-   grid whose warps take members from a work queue, so files of very uneven
-   sizes share the GPU without a tail per file;
+2. ONE ``cb_inflate`` call inflates the members of all files: persistent
+   grids whose lanes (decode) and warps (copy) take members from work queues,
+   so files of very uneven sizes share the GPU without a tail per file;
 3. per file, ``cb_record_chain`` over the records area (header skipped), then
-   the fixed columns and the requested tags in one aux walk.
+   one record pass (``cb_decode_columns``) for the fixed columns and the
+   requested tags.
 
 The records and columns of a file equal the concatenation of the batches of
 ``read_bam`` over the same file (records never depend on the chunking; only
