@@ -26,7 +26,7 @@ from dataclasses import dataclass, field
 
 import torch
 
-from cubam_b200 import _lib
+from cubam_b200 import _lib, _trace
 from cubam_b200.bam import _TYPES, FIELDS, BamHeader, Tag
 from cubam_b200.bgzf import (
     ctypes_sizeof,
@@ -117,8 +117,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
 
     With ``derived`` the columns also hold ``aligned_length`` and ``name_hash``, computed in the
     same pass over the records as the fixed fields."""
-    if events:
-        events.mark("start")
+    _trace.mark(events, "start")
     scans = []
     for comp, _ in files:
         n = int(comp.numel())
@@ -161,8 +160,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
         job_lists.append(j)
         base += int(info.total_out)
     all_jobs = torch.cat(job_lists) if len(job_lists) > 1 else job_lists[0]
-    if events:
-        events.mark("scanned")
+    _trace.mark(events, "scanned")
     inflate_summ = torch.zeros(ctypes_sizeof(_lib.InflateSummary), dtype=torch.uint8, device="cuda")
     if n_jobs:
         qws = torch.empty(inflate_workspace_bytes(n_jobs, total), dtype=torch.uint8, device="cuda")
@@ -170,8 +168,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
         del qws
         if counter is not None:
             counter["launches"] = counter.get("launches", 0) + inflate_launches(0, n_jobs)
-    if events:
-        events.mark("inflated")
+    _trace.mark(events, "inflated")
     chains = []
     base = 0
     for (comp, header), info in zip(files, infos):
@@ -190,8 +187,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
             if counter is not None:
                 counter["launches"] = counter.get("launches", 0) + KERNELS["chain"]
         chains.append((data, offsets, csumm))
-    if events:
-        events.mark("chained")
+    _trace.mark(events, "chained")
     sums = torch.stack([c[2] for c in chains]).cpu().numpy()  # one sync for all files
     raise_status(read_struct(inflate_summ, _lib.InflateSummary).status, "inflate")
     results = []
@@ -224,8 +220,7 @@ def decode_many(files: list[tuple[torch.Tensor, BamHeader]], tags=("CB", "UB", "
             if counter is not None:
                 counter["launches"] = counter.get("launches", 0) + KERNELS["records"]
         results.append(DecodedFile(header, data, off, cols, tag_cols, int(info.n_members), int(info.total_out)))
-    if events:
-        events.mark("decoded")
+    _trace.mark(events, "decoded")
     return results
 
 
@@ -337,16 +332,14 @@ class BatchPlan:
         """Issue the whole batch on the current stream (no host synchronisation)."""
         form = form or self.form or 0
         s = stream_ptr()
-        if events:
-            events.mark("start")
+        _trace.mark(events, "start")
         for k, ((comp, _), n) in enumerate(zip(self.files, [int(c.numel()) for c, _ in self.files])):
             jp = self.jobs.data_ptr() + self.job_base[k] * _lib.JOB_BYTES
             rc = _lib.lib.cb_scan_members(comp.data_ptr() if n else None, n, 1, self.out_base[k], jp,
                                           self.n_jobs[k], self.scan_summ[k].data_ptr(), self.scan_ws.data_ptr(),
                                           self.scan_ws.numel(), s)
             _lib.check(rc, "cb_scan_members")
-        if events:
-            events.mark("scanned")
+        _trace.mark(events, "scanned")
         need = inflate_workspace_bytes(self.job_base[-1], self.total_out, form)
         if self.queue_ws is None or self.queue_ws.numel() < need:
             if self.graph is not None:
@@ -356,8 +349,7 @@ class BatchPlan:
               else self.queue_ws[: int(_lib.lib.cb_inflate_workspace_bytes())])
         launch_inflate(self.jobs.data_ptr(), self.job_base[-1], self.out.data_ptr(), self.total_out, self.check_crc,
                        self.inflate_summ.data_ptr(), ws, form)
-        if events:
-            events.mark("inflated")
+        _trace.mark(events, "inflated")
         for k, ((comp, header), data, off, nrec) in enumerate(zip(self.files, self.data, self.offsets,
                                                                    self.n_records)):
             n = int(data.numel())
@@ -366,8 +358,7 @@ class BatchPlan:
                                               self.chain_summ[k].data_ptr(), self.chain_ws.data_ptr(),
                                               self.chain_ws.numel(), s)
                 _lib.check(rc, "cb_record_chain")
-        if events:
-            events.mark("chained")
+        _trace.mark(events, "chained")
         for k, (res, arrs, nrec) in enumerate(zip(self.results, self._tag_arrays, self.n_records)):
             if not nrec:
                 continue
@@ -378,8 +369,7 @@ class BatchPlan:
                                             "".join(self.tags).encode(), k,
                                             *((a.data_ptr() for a in arrs) if k else (None,) * 4), s)
             _lib.check(rc, "cb_decode_columns")
-        if events:
-            events.mark("decoded")
+        _trace.mark(events, "decoded")
 
     def launches_per_run(self) -> int:
         """Kernels of this library in one :meth:`launch` (the graph holds the same)."""

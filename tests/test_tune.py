@@ -52,3 +52,34 @@ def test_unreadable_cache_is_empty(tmp_path):
 def test_pow2_rounding():
     assert tune._pow2(1) == 1 and tune._pow2(0) == 1
     assert tune._pow2(60000) == 65536 and tune._pow2(40000) == 32768
+
+
+def test_nvtx_stage_ranges(monkeypatch):
+    """Stage boundaries open and close one NVTX range per stage when tracing is on, none when off."""
+    from cubam_b200 import _trace
+
+    calls = []
+
+    class FakeNvtx:
+        def range_push(self, name):
+            calls.append(("push", name))
+
+        def range_pop(self):
+            calls.append(("pop",))
+
+    monkeypatch.setattr(_trace, "_nvtx", lambda: FakeNvtx())
+    marked = []
+
+    class Events:
+        def mark(self, name):
+            marked.append(name)
+
+    for name in ("start", "scanned", "inflated", "chained", "decoded"):
+        _trace.mark(Events(), name, enabled=True)
+    assert marked == ["start", "scanned", "inflated", "chained", "decoded"]
+    assert [c[0] for c in calls] == ["push", "pop", "push", "pop", "push", "pop", "push", "pop"]
+    assert [c[1] for c in calls if c[0] == "push"] == ["cubam: member scan", "cubam: inflate", "cubam: record chain",
+                                                       "cubam: record pass"]
+    calls.clear()
+    _trace.mark(None, "start", enabled=False)
+    assert calls == []
