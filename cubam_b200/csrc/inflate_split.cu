@@ -128,19 +128,56 @@ __host__ __device__ __forceinline__ unsigned long long slot_bytes(uint32_t isize
 constexpr int SLOT_NT = 1024;
 __global__ void __launch_bounds__(SLOT_NT) k_slots(const cb_member_job* __restrict__ jobs, int64_t n_jobs,
                                                    const int64_t* __restrict__ d_n_jobs, uint8_t* ws) {
-    __shared__ unsigned long long sm[33];
+    // Each warp takes a contiguous segment of jobs, read coalesced with eight loads per lane in
+    // flight: a first pass sums the segment's slots, the warps' sums are scanned, a second pass
+    // writes the slot offsets.
+    constexpr int NW = SLOT_NT / 32, U = 8;
+    __shared__ unsigned long long wbase[NW + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     long long n = n_jobs;
     if (d_n_jobs) n = min((long long)n, (long long)*d_n_jobs);
-    const long long per = (n + SLOT_NT - 1) / SLOT_NT;
-    const long long a = min((long long)threadIdx.x * per, n), b = min(a + per, n);
+    const long long seg = ((n + NW - 1) / NW + 32 * U - 1) / (32 * U) * (32 * U);
+    const long long a = min((long long)warp * seg, n), b = min(a + seg, n);
     unsigned long long sum = 0;
-    for (long long j = a; j < b; j++) sum += slot_bytes(jobs[j].isize);
-    unsigned long long total;
-    unsigned long long off = block_exclusive_scan<SLOT_NT>(sum, total, sm);
+    for (long long j0 = a; j0 < b; j0 += 32 * U) {
+        uint32_t isz[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long j = j0 + k * 32 + lane;
+            isz[k] = j < b ? jobs[j].isize : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) sum += j0 + k * 32 + lane < b ? (unsigned long long)slot_bytes(isz[k]) : 0ull;
+    }
+    for (int d = 16; d; d >>= 1) sum += __shfl_xor_sync(FULL, sum, d);
+    if (lane == 0) wbase[warp] = sum;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned long long x = lane < NW ? wbase[lane] : 0ull;
+        unsigned long long tot;
+        const unsigned long long e = warp_exclusive_scan(x, tot);
+        __syncwarp();
+        if (lane < NW) wbase[lane] = e;
+    }
+    __syncthreads();
     unsigned long long* slot = reinterpret_cast<unsigned long long*>(ws + WS_HEAD);
-    for (long long j = a; j < b; j++) {
-        slot[2 * j + 1] = off;
-        off += slot_bytes(jobs[j].isize);
+    unsigned long long carry = wbase[warp];
+    for (long long j0 = a; j0 < b; j0 += 32 * U) {
+        uint32_t isz[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long j = j0 + k * 32 + lane;
+            isz[k] = j < b ? jobs[j].isize : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const long long j = j0 + k * 32 + lane;
+            const unsigned long long v = j < b ? (unsigned long long)slot_bytes(isz[k]) : 0ull;
+            unsigned long long t;
+            const unsigned long long x = warp_exclusive_scan(v, t);
+            if (j < b) slot[2 * j + 1] = carry + x;
+            carry += t;
+        }
     }
 }
 

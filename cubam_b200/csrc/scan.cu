@@ -109,8 +109,19 @@ __device__ __forceinline__ uint32_t chunk_mask(const uint8_t* buf, long long n, 
         while (eq) {
             const int t = (__ffs(eq) - 1) >> 3;
             eq &= ~(0xffu << (8 * t));
-            const long long o = start + 4 * k + t;
-            if (member_at(buf, n, o)) mask |= 1u << (4 * k + t);
+            const int q = 4 * k + t;  // the byte's place in the chunk
+            if (q <= 12) {
+                // the next three header bytes (8b 08 04) are in this chunk: test them from the registers
+                // first (the chunk as a 128-bit value shifted right by q + 1 bytes), so that most 0x1f
+                // bytes need no further load
+                const unsigned sh = 8u * (unsigned)(q + 1);  // 8..104
+                const unsigned long long lo = (unsigned long long)w[0] | ((unsigned long long)w[1] << 32);
+                const unsigned long long hi = (unsigned long long)w[2] | ((unsigned long long)w[3] << 32);
+                const unsigned long long x = sh < 64 ? (lo >> sh) | (hi << (64 - sh)) : hi >> (sh - 64);
+                if ((x & 0xFFFFFFull) != 0x04088Bull) continue;
+            }
+            const long long o = start + q;
+            if (member_at(buf, n, o)) mask |= 1u << q;
         }
     }
     return mask;
