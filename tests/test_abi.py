@@ -69,3 +69,41 @@ def test_launch_parameters_are_checked_and_restored():
                          (_lib.PARAM_SPLIT_MIN_JOBS, 8192), (_lib.PARAM_COPY_UNITS, 2),
                          (_lib.PARAM_DECODE_PIPELINE, 1)):
         assert L.cb_get_param(key) == default
+
+
+def test_header_compiles_as_c_and_a_c_program_links(tmp_path):
+    """include/cubam_b200.h is plain C99, and a C program links the library and calls it (entry points
+    that need no GPU: the version, the launch parameters, the workspace sizes)."""
+    import shutil
+    import subprocess
+
+    from cubam_b200 import _lib
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        import pytest
+
+        pytest.skip("no C compiler")
+    src = tmp_path / "use.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "cubam_b200.h"
+int main(void) {
+    cb_batch* none = 0;
+    (void)none;
+    if (cb_get_param(CB_PARAM_INFLATE_FORM) != 3) return 2;
+    if (cb_set_param(CB_PARAM_DECODE_ROOT, 6) != CB_OK || cb_get_param(CB_PARAM_DECODE_ROOT) != 6) return 3;
+    if (cb_set_param(CB_PARAM_DECODE_ROOT, 9) != CB_ERR_ARG) return 4;
+    if (cb_scan_workspace_bytes(1 << 20) == 0 || cb_record_chain_workspace_bytes(1 << 20) == 0) return 5;
+    if (cb_inflate_split_workspace_bytes(10, 655360) < 2 * 655360) return 6;
+    printf("%s\n", cb_version());
+    return 0;
+}
+''')
+    exe = tmp_path / "use"
+    libdir = Path(_lib.LIB_PATH).parent
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", str(ROOT / "include"), str(src), "-o", str(exe),
+                    "-L", str(libdir), "-lcubam_b200", f"-Wl,-rpath,{libdir}"], check=True, capture_output=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    assert r.stdout.strip()
