@@ -89,3 +89,23 @@ def test_install_refuses_another_cubam(shim, monkeypatch, tmp_path):
     monkeypatch.setitem(sys.modules, "cubam", fake)
     with pytest.raises(RuntimeError, match="already imported"):
         compat.install()
+
+
+def test_launch_arguments_from_cupy_style_objects(shim):
+    """cubam passes CuPy arrays and NumPy scalars: arrays become their device pointers through
+    __cuda_array_interface__, scalars become integers, and a host tensor is refused."""
+    import numpy as np
+    import torch
+
+    shim()
+    import cubam._kernels as k
+
+    class CupyLike:
+        def __init__(self, ptr):
+            self.__cuda_array_interface__ = {"data": (ptr, False), "shape": (4,), "typestr": "|u1", "version": 3}
+
+    assert k._arg(CupyLike(0x7F0000001000)) == 0x7F0000001000
+    assert k._arg(np.int64(12)) == 12 and k._arg(np.uint8(ord("C"))) == 67
+    assert k._arg(None) is None
+    with pytest.raises(TypeError, match="GPU"):
+        k._arg(torch.zeros(4))
