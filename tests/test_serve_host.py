@@ -68,3 +68,108 @@ def test_timeout_status_raises_timeout_error():
         raise_status(_lib.TIMEOUT, "request 3")
     with pytest.raises(ValueError, match="Too many candidates"):
         raise_status(_lib.TOO_MANY, "scan")
+
+
+# ---- step planning on a member index held on the host
+
+def _fake_file(n_members=400, seed=3):
+    """A resident file's index without its bytes: members of 15-30 KB compressed holding 65,280 inflated
+    bytes; no record starts in about one member of ten (a long record crosses it)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    csz = rng.integers(15_000, 30_000, n_members)
+    coff = np.concatenate([[0], np.cumsum(csz)]).astype(np.int64)
+    ucum = (np.arange(n_members + 1) * 65280).astype(np.int64)
+    first = rng.integers(0, 300, n_members + 1).astype(np.int64)
+    first[rng.random(n_members + 1) < 0.1] = -1
+    first[0], first[n_members] = 0, 0
+    counts = rng.integers(200, 260, n_members)
+    cum = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    rf = serve.ResidentFile.__new__(serve.ResidentFile)
+    rf.index = serve.MemberIndex(coff, ucum, first, cum, np.zeros((n_members, 4), np.int64))
+    return rf
+
+
+def _request(rf, a, b, rid=0):
+    req = serve.Request(0, rf.voff(a), rf.voff(b), rid=rid)
+    serve.plan_request(rf, req)
+    return req
+
+
+def test_slices_cover_the_request_at_record_starts():
+    rf = _fake_file()
+    ok = set(rf.boundaries().tolist())
+    b = sorted(ok)
+    for a_i, b_i in ((0, len(b) - 1), (5, 40), (100, 101), (3, 3)):
+        req = _request(rf, b[a_i], b[b_i])
+        sl = serve.slice_request(rf, req, 100_000)
+        if req.m0 == req.m1:
+            assert sl == []
+            continue
+        assert sl[0][0] == req.m0 and sl[-1][1] == req.m1
+        for (x0, x1), (y0, _) in zip(sl, sl[1:]):
+            assert x1 == y0
+        for ma, mb in sl:
+            assert mb in ok and mb > ma
+            size = int(rf.index.coff[mb] - rf.index.coff[ma])
+            # at most slice_bytes, unless no record start comes sooner
+            nearer = [m for m in ok if ma < m < mb]
+            assert size <= 100_000 or not nearer
+
+
+def _planner(rf, step_bytes, short_bytes, small_bytes):
+    s = serve.Server.__new__(serve.Server)
+    s.files = [rf]
+    s.long_step_bytes, s.short_step_bytes, s.small_bytes = step_bytes, short_bytes, small_bytes
+    s.step_bytes = step_bytes
+    s.slice_bytes = 100_000
+    s.pending, s.active = [], []
+    return s
+
+
+def _admit(s, req):
+    req._slices = serve.slice_request(s.files[0], req, s.slice_bytes)
+    req._next = 0
+    s.active.append(req)
+
+
+def test_steps_keep_their_size_and_serve_the_oldest_first():
+    rf = _fake_file()
+    b = rf.boundaries()
+    s = _planner(rf, step_bytes=1_000_000, short_bytes=300_000, small_bytes=50_000)
+    big = [_request(rf, int(b[i]), int(b[i + 60]), rid=i) for i in (0, 100, 200)]
+    for r in big:
+        _admit(s, r)
+    seen_slices = {r.rid: 0 for r in big}
+    for _ in range(200):
+        step = s._pick()
+        if not step:
+            break
+        assert step[0].req is s.active[0] or step[0].req._next > 0  # the oldest request is served first
+        total = sum(int(rf.index.coff[x.mb] - rf.index.coff[x.ma]) for x in step)
+        assert total <= s.step_bytes or len(step) == 1
+        assert s.step_bytes == 1_000_000  # no small request waits
+        for x in step:
+            seen_slices[x.req.rid] += 1
+            if x.last:
+                assert x.req._last_launched
+        s.active = [r for r in s.active if not r._last_launched]
+    assert not s.active  # every request got all its slices
+
+
+def test_a_waiting_small_request_shortens_the_steps():
+    rf = _fake_file()
+    b = rf.boundaries()
+    s = _planner(rf, step_bytes=1_000_000, short_bytes=300_000, small_bytes=50_000)
+    _admit(s, _request(rf, int(b[0]), int(b[150]), rid=1))
+    small = _request(rf, int(b[200]), int(b[201]), rid=2)
+    assert small.compressed_bytes <= 50_000
+    s.pending.append(small)  # arrived, not admitted yet
+    step = s._pick()
+    assert s.step_bytes == 300_000
+    assert sum(int(rf.index.coff[x.mb] - rf.index.coff[x.ma]) for x in step) <= 300_000 or len(step) == 1
+    s.pending.clear()
+    _admit(s, small)
+    step = s._pick()
+    assert any(x.req is small for x in step)  # a started small request goes in the next step
