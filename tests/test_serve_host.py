@@ -173,3 +173,30 @@ def test_a_waiting_small_request_shortens_the_steps():
     _admit(s, small)
     step = s._pick()
     assert any(x.req is small for x in step)  # a started small request goes in the next step
+
+
+def test_pool_allocator_never_overlaps_and_coalesces():
+    import random
+
+    rng = random.Random(5)
+    pool = serve.PoolAllocator(1 << 24)
+    live = {}
+    for step in range(4000):
+        if live and (rng.random() < 0.45 or pool.available() < (1 << 20)):
+            off = rng.choice(list(live))
+            pool.release(off, live.pop(off))
+        else:
+            n = rng.choice([1, 255, 256, 257, 4096, 100_000, 1 << 20])
+            off = pool.alloc(n)
+            if off is None:
+                continue
+            assert off % 256 == 0
+            live[off] = n
+        spans = sorted((o, o + ((n + 255) & ~255 or 256)) for o, n in live.items())
+        for (a0, a1), (b0, _) in zip(spans, spans[1:]):
+            assert a1 <= b0  # no two live ranges overlap
+        assert all(a1 <= (1 << 24) for _, a1 in spans)
+        assert pool.available() + sum(a1 - a0 for a0, a1 in spans) == 1 << 24
+    for off, n in list(live.items()):
+        pool.release(off, n)
+    assert pool.free == [(0, 1 << 24)]
